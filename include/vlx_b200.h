@@ -1,0 +1,137 @@
+/*
+ * vlx_b200 — B200-native four-centre Fock build, C ABI.
+ *
+ * Drop-in replacement for the compute calls of the reference's Fock-build path
+ * (VeloxChem): plain pointers and sizes, no C++ or framework types.  Matrices
+ * are dense, row-major, nao x nao FP64 in the reference AO order
+ * (CMolecularBasis::index_map: all functions of angular momentum l after those
+ * of l - 1; inside l, index = offset_l + m * N_l + s, m = 0..2l for real solid
+ * harmonics m = -l..l, s the running index of l-shells over atoms).
+ *
+ * Every entry point returns VLX_B200_OK (0) or an error code and never aborts;
+ * vlx_b200_last_error() gives the message of the last failure on the calling
+ * thread.  A screener is not safe for concurrent calls from several threads
+ * (it owns the device scratch buffers of its builds).
+ */
+#ifndef VLX_B200_H
+#define VLX_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLX_B200_OK 0
+#define VLX_B200_ERR_ARGUMENT 1    /* invalid argument (null pointer, size, label) */
+#define VLX_B200_ERR_CUDA 2        /* CUDA runtime error (message has the details) */
+#define VLX_B200_ERR_UNSUPPORTED 3 /* angular momentum or option not compiled in */
+#define VLX_B200_ERR_NO_DEVICE 4   /* no CUDA device available */
+
+typedef struct vlx_b200_screener vlx_b200_screener;
+
+/* Statistics of one build (any field may be ignored by passing NULL). */
+typedef struct {
+    double device_ms;          /* device time of the integral + digestion kernels */
+    double total_ms;           /* wall time of the call, including copies */
+    long long shell_quartets;  /* unique shell quartets evaluated */
+    long long prim_quartets;   /* primitive quartets evaluated */
+    long long kernel_launches; /* kernels launched by the call */
+} vlx_b200_stats;
+
+/* Library version string. */
+const char* vlx_b200_version(void);
+
+/* Message of the last error raised on the calling thread ("" if none). */
+const char* vlx_b200_last_error(void);
+
+/* Number of visible CUDA devices. */
+int vlx_b200_device_count(int* count);
+
+/* Normalises one contracted shell in place (raw coefficients in, normalised
+ * primitive factors out).
+ * Replaces CBasisFunction::normalize (src/orbdata/BasisFunction.cpp:129-146). */
+int vlx_b200_normalize_shell(int l, int nprim, const double* exponents, double* coefficients);
+
+/* Builds the shell-pair data of a molecule on `device`, evaluates the Schwarz
+ * diagonals (ab|ab) on the GPU and bins the pairs into 16 decades.
+ * xyz: natoms x 3 coordinates in bohr.  Shells in the reference order (atom by
+ * atom, basis-file order): shell_atom, shell_l, shell_nprim per shell;
+ * exponents / coefficients concatenated over shells, raw coefficients.
+ * Replaces CT4CScreener::partition(basis, molecule, "eri")
+ * (src/t4c_func/T4CScreener.cpp:63-119; bins: BlockedGtoPairBlock.cpp:22-42). */
+int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, const double* xyz, int nshells,
+                             const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                             const double* exponents, const double* coefficients);
+
+/* Releases a screener and its device memory. */
+int vlx_b200_screener_destroy(vlx_b200_screener* screener);
+
+/* Number of spherical basis functions. */
+int vlx_b200_screener_nao(const vlx_b200_screener* screener, int* nao);
+
+/* Number of shell pairs (all pair blocks, screened-out pairs included). */
+int vlx_b200_screener_npairs(const vlx_b200_screener* screener, int* npairs);
+
+/* Per shell pair, in the reference pair order (pair blocks over GTO blocks
+ * (l, nprim) i <= j; inside a diagonal block column-wise upper triangle):
+ * info[6*p..6*p+5] = {pair block, bin (-1 = dropped), la, lb, AO index of A,
+ * AO index of B}, maxv[p] = max over components of (ab|ab).
+ * Replaces CT4CScreener::gto_pair_blocks (T4CScreener.cpp:257-260). */
+int vlx_b200_screener_pair_info(const vlx_b200_screener* screener, int* info, double* maxv);
+
+/* Block-size knob of the reference (CFockDriver::set_block_size_factor,
+ * src/t4c_func/FockDriver.cpp:356-360): here the number of ket pairs of one
+ * GPU work item is 256 / factor, at least 32. */
+int vlx_b200_set_block_size_factor(vlx_b200_screener* screener, int factor);
+
+/* One Fock matrix.  density / fock_out: host nao x nao.  symmetric != 0 for a
+ * symmetric density (reference mat_t::symmetric), else general.
+ * label: "2jk", "2jkx", "j", "k", "kx" ("j_rs", "k_rs", "kx_rs" alias the
+ * last three); an unknown label yields a zero matrix, as in the reference.
+ * omega must be 0 (range-separated integrals are not compiled in).
+ * Quartets with bin(bra) + bin(ket) <= ithreshold are included.
+ * Replaces CFockDriver::compute(screener, density, label, exchange_factor,
+ * omega, ithreshold) (src/t4c_func/FockDriver.cpp:120-172). */
+int vlx_b200_fock_build(vlx_b200_screener* screener, const double* density, int symmetric, const char* label,
+                        double exchange_factor, double omega, int ithreshold, double* fock_out,
+                        vlx_b200_stats* stats);
+
+/* The share of the build of rank `rank` out of `nodes` (work items dealt
+ * round-robin); the sum over ranks equals vlx_b200_fock_build.
+ * Replaces CFockDriver::compute(screener, rank, nodes, density, ...)
+ * (src/t4c_func/FockDriver.cpp:234-290). */
+int vlx_b200_fock_build_local(vlx_b200_screener* screener, int rank, int nodes, const double* density,
+                              int symmetric, const char* label, double exchange_factor, double omega,
+                              int ithreshold, double* fock_out, vlx_b200_stats* stats);
+
+/* Several densities, one label each, in one pass over the quartets.
+ * densities / focks_out: ndens host matrices of nao x nao.
+ * Replaces CFockDriver::compute(screener, densities, labels, ...)
+ * (src/t4c_func/FockDriver.cpp:176-230) and its rank/nodes overload (:294-352)
+ * when nodes > 1. */
+int vlx_b200_fock_build_multi(vlx_b200_screener* screener, int rank, int nodes, int ndens,
+                              const double* const* densities, int symmetric, const char* const* labels,
+                              double exchange_factor, double omega, int ithreshold, double* const* focks_out,
+                              vlx_b200_stats* stats);
+
+/* Device-resident build: d_density and d_fock are device pointers (nao x nao)
+ * on the screener's device; stream is a cudaStream_t (NULL = the screener's
+ * own stream).  Returns when the work is enqueued; stats->device_ms is 0. */
+int vlx_b200_fock_build_device(vlx_b200_screener* screener, const double* d_density, int symmetric,
+                               const char* label, double exchange_factor, double omega, int ithreshold,
+                               double* d_fock, void* stream);
+
+/* Dense (nao)^4 ERI tensor over the screened unique quartets (all eight
+ * index permutations written), host buffer.
+ * Replaces CFockDriver::compute_eri(screener, nao, ithreshold)
+ * (src/t4c_func/FockDriver.cpp:76-117). */
+int vlx_b200_compute_eri(vlx_b200_screener* screener, int ithreshold, double* eri_out);
+
+/* Boys function F_m(T) for n arguments as the device evaluates it
+ * (host arrays T[n] in, F[n] out), for validation. */
+int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VLX_B200_H */

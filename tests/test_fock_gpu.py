@@ -1,0 +1,205 @@
+"""Parity of the CUDA Fock build (through the C ABI) with the oracle and the
+reference's golden matrices.  Tolerances: J, K and 2J-K to 1e-10 absolute
+(max element), ERI tensors to 1e-12, Schwarz values to 1e-12 relative."""
+
+import json
+import pickle
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _fock(screener, dense, label, xfac=1.0, ith=15, symmetric=True, rank=0, nodes=1):
+    from veloxchem_b200 import FockDriver, make_matrix, mat_t
+    drv = FockDriver((rank, nodes))
+    m = make_matrix(screener._basis, mat_t.symmetric if symmetric else mat_t.general)
+    m.set_values(dense)
+    return drv.compute(screener, m, label, xfac, 0.0, ith).full_matrix().to_numpy()
+
+
+def _screener(mol, bas):
+    from veloxchem_b200 import T4CScreener
+    s = T4CScreener()
+    s.partition(bas, mol, 'eri')
+    s._basis = bas
+    return s
+
+
+def test_boys_device_against_oracle():
+    from oracle.oracle import PortOracle
+    from veloxchem_b200 import _native
+    t = np.concatenate([np.linspace(0.0, 45.0, 901), [1e-12, 39.999999, 40.0, 60.0, 120.0, 700.0]])
+    for m in range(0, 17):
+        dev = _native.boys_device(m, t)
+        ref = np.array([PortOracle.boys(m, x) for x in t])
+        assert np.max(np.abs(dev - ref) / np.maximum(ref, 1e-300)) < 5e-14, m
+
+
+def test_screener_known_answers_and_bins():
+    from oracle.oracle import PortOracle
+    kat = json.loads((GOLDEN / 'screener_sto3g.json').read_text())
+    g, mol, bas = load_golden('h2o_sto3g.npz')
+    s = _screener(mol, bas)
+    info, maxv = s.pair_info()
+    for blk, key in enumerate(['ss', 'sp', 'pp']):
+        assert np.allclose(maxv[info[:, 0] == blk], kat[key], rtol=1e-12, atol=1e-14)
+    oinfo, omax = PortOracle(mol, bas).pair_info()
+    assert np.array_equal(info, oinfo)
+
+
+def test_screener_pickle_roundtrip():
+    g, mol, bas = load_golden('h2o_sto3g.npz')
+    a = _screener(mol, bas)
+    b = pickle.loads(pickle.dumps(a))
+    assert a == b
+
+
+def test_eri_tensor_sto3g_golden():
+    from veloxchem_b200 import FockDriver
+    g, mol, bas = load_golden('h2o_sto3g.npz')
+    eri = FockDriver().compute_eri(mol, bas)
+    assert np.max(np.abs(eri - g['eri'])) < 1e-12
+
+
+@pytest.mark.parametrize('basis', ['def2-svp', 'def2-tzvp'])
+def test_eri_tensor_every_class(basis):
+    """All quartet classes of the basis (compiled and table-driven) against
+    the oracle's ERI tensor, on one water molecule."""
+    from oracle.oracle import PortOracle
+    from veloxchem_b200 import FockDriver, MolecularBasis, Molecule
+    mol = Molecule.read_str('O 0.1 -0.05 0.02\nH 0.0 0.76 0.59\nH -0.02 -0.74 0.61')
+    bas = MolecularBasis.read(mol, basis)
+    eri = FockDriver().compute_eri(mol, bas, 1e-15)
+    ref = PortOracle(mol, bas).eri(15)
+    assert np.max(np.abs(eri - ref)) < 1e-12
+
+
+@pytest.mark.parametrize('name', ['h2o_sto3g.npz', 'h2o_dimer_svpd.npz', 'h2o_dimer_tzvp.npz'])
+def test_jk_against_reference_goldens(name):
+    g, mol, bas = load_golden(name)
+    s = _screener(mol, bas)
+    j = _fock(s, g['density'], 'j', 0.0)
+    k = _fock(s, g['density'], 'k', 0.0)
+    f = _fock(s, g['density'], '2jk', 0.0)
+    assert np.max(np.abs(j - g['j'])) < TOL
+    assert np.max(np.abs(k - g['k'])) < TOL
+    assert np.max(np.abs(f - (2 * g['j'] - g['k']))) < TOL
+
+
+def test_general_density_against_goldens():
+    g, mol, bas = load_golden('h2o_dimer_svpd.npz')
+    s = _screener(mol, bas)
+    j = _fock(s, g['density_gen'], 'j', 0.0, symmetric=False)
+    k = _fock(s, g['density_gen'], 'k', 0.0, symmetric=False)
+    assert np.max(np.abs(j - g['j_gen'])) < TOL
+    assert np.max(np.abs(k - g['k_gen'].T)) < TOL
+
+
+@pytest.mark.parametrize('label,xfac', [('2jk', 1.0), ('2jkx', 0.28), ('j', 1.0), ('k', 1.0), ('kx', 0.73)])
+def test_labels_against_oracle(label, xfac):
+    from oracle.oracle import PortOracle
+    g, mol, bas = load_golden('h2o_dimer_tzvp.npz')
+    s = _screener(mol, bas)
+    ref = PortOracle(mol, bas).fock(g['density'], label, xfac, 15)
+    assert np.max(np.abs(_fock(s, g['density'], label, xfac) - ref)) < TOL
+
+
+def test_unknown_label_gives_zero_matrix():
+    g, mol, bas = load_golden('h2o_sto3g.npz')
+    s = _screener(mol, bas)
+    assert np.all(_fock(s, g['density'], 'nonsense', 0.0) == 0.0)
+
+
+def test_cluster_fixture_ithreshold12():
+    """(H2O)_4 / def2-SVP, seeded density, against the compiled reference."""
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    assert np.max(np.abs(_fock(s, g['density'], 'j', 1.0, 12) - g['j'])) < TOL
+    assert np.max(np.abs(_fock(s, g['density'], 'k', 1.0, 12) - g['k'])) < TOL
+    assert np.max(np.abs(_fock(s, g['density'], '2jk', 1.0, 12) - g['f2jk'])) < TOL
+
+
+@pytest.mark.parametrize('ith', [4, 8, 10])
+def test_loose_thresholds_match_oracle(ith):
+    """The screening rule (bin sums) at thresholds that drop many quartets."""
+    from oracle.oracle import PortOracle
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    ref = PortOracle(mol, bas).fock(g['density'], '2jk', 1.0, ith)
+    assert np.max(np.abs(_fock(s, g['density'], '2jk', 1.0, ith) - ref)) < TOL
+
+
+def test_rank_partition_sums_to_full_build():
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    full = _fock(s, g['density'], '2jk', 1.0, 12)
+    parts = [_fock(s, g['density'], '2jk', 1.0, 12, rank=r, nodes=3) for r in range(3)]
+    assert np.max(np.abs(sum(parts) - full)) < 1e-12
+    assert all(np.max(np.abs(p)) > 0 for p in parts)
+
+
+def test_multi_density_overload():
+    from veloxchem_b200 import FockDriver, Matrices, make_matrix, mat_t
+    g, mol, bas = load_golden('h2o_dimer_svpd.npz')
+    s = _screener(mol, bas)
+    dm = make_matrix(bas, mat_t.general)
+    dm.set_values(g['density_gen'])
+    dens = Matrices()
+    dens.add(dm, '0')
+    dens.add(dm, '1')
+    out = FockDriver().compute(s, dens, ['j', 'k'], 0.0, 0.0, 15)
+    assert np.max(np.abs(out.matrix('0').full_matrix().to_numpy() - g['j_gen'])) < TOL
+    assert np.max(np.abs(out.matrix('1').full_matrix().to_numpy() - g['k_gen'].T)) < TOL
+
+
+def test_block_size_factor_does_not_change_result():
+    from veloxchem_b200 import FockDriver, make_matrix, mat_t
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    drv = FockDriver()
+    m = make_matrix(bas, mat_t.symmetric)
+    m.set_values(g['density'])
+    a = drv.compute(s, m, '2jk', 1.0, 0.0, 12).full_matrix().to_numpy()
+    drv._set_block_size_factor(8)
+    b = drv.compute(s, m, '2jk', 1.0, 0.0, 12).full_matrix().to_numpy()
+    assert np.max(np.abs(a - b)) < 1e-12
+
+
+def test_omega_is_rejected_loudly():
+    from veloxchem_b200._native import NativeError
+    g, mol, bas = load_golden('h2o_sto3g.npz')
+    s = _screener(mol, bas)
+    from veloxchem_b200 import FockDriver, make_matrix, mat_t
+    m = make_matrix(bas, mat_t.symmetric)
+    m.set_values(g['density'])
+    with pytest.raises(NativeError):
+        FockDriver().compute(s, m, 'kx_rs', 1.0, 0.3, 15)
+
+
+def test_large_cluster_properties():
+    """(H2O)_32 / def2-SVP at ithreshold 12 (the bench workload): size-independent
+    checks -- F symmetric, J positive semidefinite energy, linearity in D."""
+    from veloxchem_b200.geometry import CLUSTERS, random_density, water_cluster
+    from veloxchem_b200 import MolecularBasis
+    lattice, seed = CLUSTERS['h2o32']
+    mol = water_cluster(lattice, seed)
+    bas = MolecularBasis.read(mol, 'def2-svp')
+    s = _screener(mol, bas)
+    assert s.nao == 768
+    d1 = random_density(768, 160, 1)
+    d2 = random_density(768, 160, 2)
+    j1 = _fock(s, d1, 'j', 1.0, 12)
+    j2 = _fock(s, d2, 'j', 1.0, 12)
+    j12 = _fock(s, d1 + 0.5 * d2, 'j', 1.0, 12)
+    assert np.max(np.abs(j12 - (j1 + 0.5 * j2))) < 1e-9
+    assert np.max(np.abs(j1 - j1.T)) < 1e-12
+    assert np.sum(d1 * j1) > 0
+    k1 = _fock(s, d1, 'k', 1.0, 12)
+    f1 = _fock(s, d1, '2jk', 1.0, 12)
+    assert np.max(np.abs(f1 - (2 * j1 - k1))) < 1e-9

@@ -1,0 +1,115 @@
+"""ctypes binding of the C ABI in include/vlx_b200.h (libvlx_b200.so).
+
+The library is built in-tree (python -m veloxchem_b200.build).  There is no
+fallback: if the library is missing or fails to load, every entry point raises.
+"""
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / 'lib' / 'libvlx_b200.so'
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes); every symbol declared in include/vlx_b200.h
+SIGNATURES = {
+    'vlx_b200_version': (ctypes.c_char_p, []),
+    'vlx_b200_last_error': (ctypes.c_char_p, []),
+    'vlx_b200_device_count': (ctypes.c_int, [_ip]),
+    'vlx_b200_normalize_shell': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    'vlx_b200_screener_create': (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                                _ip, _ip, _ip, _dp, _dp]),
+    'vlx_b200_screener_destroy': (ctypes.c_int, [_vp]),
+    'vlx_b200_screener_nao': (ctypes.c_int, [_vp, _ip]),
+    'vlx_b200_screener_npairs': (ctypes.c_int, [_vp, _ip]),
+    'vlx_b200_screener_pair_info': (ctypes.c_int, [_vp, _ip, _dp]),
+    'vlx_b200_set_block_size_factor': (ctypes.c_int, [_vp, ctypes.c_int]),
+    'vlx_b200_fock_build': (ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, _dp, _vp]),
+    'vlx_b200_fock_build_local': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int,
+                                                 ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                 _dp, _vp]),
+    'vlx_b200_fock_build_multi': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(_dp), ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_char_p), ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_int, ctypes.POINTER(_dp), _vp]),
+    'vlx_b200_fock_build_device': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    'vlx_b200_compute_eri': (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    'vlx_b200_boys_device': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+}
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [('device_ms', ctypes.c_double), ('total_ms', ctypes.c_double), ('shell_quartets', ctypes.c_longlong),
+                ('prim_quartets', ctypes.c_longlong), ('kernel_launches', ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise NativeError('native library not built: %s (run python -m veloxchem_b200.build)' % LIB_PATH)
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = lib().vlx_b200_last_error().decode(errors='replace')
+        raise NativeError('%s failed (code %d): %s' % (what, rc, msg))
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    rc = lib().vlx_b200_device_count(ctypes.byref(n))
+    return n.value if rc == 0 else 0
+
+
+def normalize_shell(l, exps, coefs):
+    e = f64(exps)
+    c = f64(coefs).copy()
+    check(lib().vlx_b200_normalize_shell(int(l), len(e), dptr(e), dptr(c)), 'normalize_shell')
+    return c
+
+
+def boys_device(m, t, device=0):
+    t = f64(t)
+    out = np.zeros_like(t)
+    check(lib().vlx_b200_boys_device(int(device), int(m), len(t), dptr(t), dptr(out)), 'boys_device')
+    return out

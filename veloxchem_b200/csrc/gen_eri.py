@@ -1,0 +1,617 @@
+"""Generator of the per-class shell-quartet recursions (CUDA device code).
+
+For a quartet class (la lb | lc ld) with la <= lb, lc <= ld the emitted code
+follows the Head-Gordon-Pople scheme the reference uses
+(src/t4c_electron_repulsion/ElectronRepulsionRec*.hpp):
+
+1. per primitive quartet, Obara-Saika vertical recursion on centres B and D
+   producing [0 e | 0 f]^(0) for |e| in [lb, la+lb], |f| in [ld, lc+ld]
+   (reference: ElectronRepulsionPrimRec*.cpp);
+2. sum over primitive quartets (reference: t2cfunc::reduce);
+3. ket horizontal recursion |c+1_i, d) = |c, d+1_i) + (D_i - C_i)|c, d)
+   (reference: ElectronRepulsionContrRecXX*.cpp);
+4. ket Cartesian -> spherical (t4cfunc::ket_transform);
+5. bra horizontal recursion (a+1_i, b| = (a, b+1_i| + (B_i - A_i)(a, b|
+   on the half-spherical data (ElectronRepulsionContrRec*XX.cpp);
+6. bra Cartesian -> spherical (t4cfunc::bra_transform).
+
+The recursion graph is built here by demand-driven expansion from the
+targets, so only the intermediates a class needs are emitted, as straight-line
+code (registers) that the compiler schedules.  Spherical factors are the real
+solid harmonics normalised with the reference's primitive normalisation
+(src/general/SphericalMomentum.hpp conventions: m = -l..l, p = (y, z, x)).
+
+Usage: python gen_eri.py OUTDIR [LMAX]
+"""
+
+import math
+import sys
+from pathlib import Path
+
+# ----------------------------------------------------------------- components
+
+def cart_list(l):
+    """Lexicographic Cartesian components of angular momentum l (xx, xy, xz, ...)."""
+    return [(x, y, l - x - y) for x in range(l, -1, -1) for y in range(l - x, -1, -1)]
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def _binom(n, k):
+    return math.comb(n, k) if 0 <= k <= n else 0
+
+
+_LNORM = {0: 1.0, 1: 2.0, 2: 2.0 / math.sqrt(3.0), 3: 4.0 / math.sqrt(15.0), 4: 2.0 / math.sqrt(105.0)}
+
+
+def _dfact(n):
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def sph_coefficients(l):
+    """rows m = -l..l, columns lexicographic Cartesian components."""
+    carts = cart_list(l)
+    idx = {c: i for i, c in enumerate(carts)}
+    rows = []
+    for m in range(-l, l + 1):
+        am = abs(m)
+        c = [0.0] * len(carts)
+        vm2 = 1 if m < 0 else 0  # 2*vm
+        for t in range((l - am) // 2 + 1):
+            for u in range(t + 1):
+                v2 = vm2
+                while v2 <= 2 * ((am - vm2) // 2) + vm2 and v2 <= am:
+                    sgn = -1.0 if ((2 * t + v2 - vm2) // 2) % 2 else 1.0
+                    coef = sgn * 0.25 ** t * _binom(l, t) * _binom(l - t, am + t) * _binom(t, u) * _binom(am, v2)
+                    px, py, pz = 2 * t + am - 2 * u - v2, 2 * u + v2, l - 2 * t - am
+                    if px >= 0 and py >= 0 and pz >= 0:
+                        c[idx[(px, py, pz)]] += coef
+                    v2 += 2
+        nrm = 0.0
+        for i, ci in enumerate(carts):
+            for j, cj in enumerate(carts):
+                s = [ci[k] + cj[k] for k in range(3)]
+                if any(v % 2 for v in s):
+                    continue
+                nrm += c[i] * c[j] * _dfact(s[0] - 1) * _dfact(s[1] - 1) * _dfact(s[2] - 1)
+        scale = 1.0 / math.sqrt(nrm * _LNORM[l] ** 2 / 4.0 ** l)
+        rows.append([v * scale for v in c])
+    return rows
+
+
+def sub1(c, i):
+    v = list(c)
+    v[i] -= 1
+    return tuple(v)
+
+
+def add1(c, i):
+    v = list(c)
+    v[i] += 1
+    return tuple(v)
+
+
+def pick_axis(c):
+    """Axis used to lower a component: the first axis (x, y, z) with the largest exponent."""
+    best = max(c)
+    for i in range(3):
+        if c[i] == best and best > 0:
+            return i
+    raise ValueError(c)
+
+
+# ----------------------------------------------------------------- VRR graph
+
+class VRR:
+    """Demand-driven OS vertical recursion for [0 e | 0 f]^(m)."""
+
+    def __init__(self):
+        self.nodes = {}   # key -> (expr terms)
+        self.order = []
+
+    def need(self, e, f, m):
+        key = (e, f, m)
+        if key in self.nodes:
+            return key
+        terms = []
+        if sum(f) > 0:
+            i = pick_axis(f)
+            f1 = sub1(f, i)
+            terms.append(('QD', i, self.need(e, f1, m)))
+            terms.append(('WQ', i, self.need(e, f1, m + 1)))
+            if f1[i] > 0:
+                f2 = sub1(f1, i)
+                terms.append(('F2', f1[i], self.need(e, f2, m), self.need(e, f2, m + 1)))
+            if e[i] > 0:
+                terms.append(('EZH', e[i], self.need(sub1(e, i), f1, m + 1)))
+        elif sum(e) > 0:
+            i = pick_axis(e)
+            e1 = sub1(e, i)
+            terms.append(('PB', i, self.need(e1, f, m)))
+            terms.append(('WP', i, self.need(e1, f, m + 1)))
+            if e1[i] > 0:
+                e2 = sub1(e1, i)
+                terms.append(('E2', e1[i], self.need(e2, f, m), self.need(e2, f, m + 1)))
+        else:
+            terms.append(('BASE', m))
+        self.nodes[key] = terms
+        self.order.append(key)
+        return key
+
+
+# ----------------------------------------------------------------- emitter
+
+AX = 'xyz'
+
+
+class ClassGen:
+    def __init__(self, la, lb, lc, ld):
+        self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
+        self.L = la + lb + lc + ld
+        self.e_targets = [c for l in range(lb, la + lb + 1) for c in cart_list(l)]
+        self.f_targets = [c for l in range(ld, lc + ld + 1) for c in cart_list(l)]
+        self.vrr = VRR()
+        for e in self.e_targets:
+            for f in self.f_targets:
+                self.vrr.need(e, f, 0)
+        self.names = {}
+        for k, key in enumerate(self.vrr.order):
+            self.names[key] = 'v%d' % k
+
+    def stats(self):
+        return dict(vrr=len(self.vrr.order), acc=len(self.e_targets) * len(self.f_targets))
+
+    def _vrr_expr(self, key):
+        terms = self.vrr.nodes[key]
+        n = self.names
+        out = []
+        for t in terms:
+            if t[0] == 'BASE':
+                return 'F[%d]' % t[1]
+            if t[0] == 'QD':
+                out.append('QD%s * %s' % (AX[t[1]], n[t[2]]))
+            elif t[0] == 'WQ':
+                out.append('WQ%s * %s' % (AX[t[1]], n[t[2]]))
+            elif t[0] == 'PB':
+                out.append('PB%s * %s' % (AX[t[1]], n[t[2]]))
+            elif t[0] == 'WP':
+                out.append('WP%s * %s' % (AX[t[1]], n[t[2]]))
+            elif t[0] == 'F2':
+                out.append('%s * hie * (%s - rh * %s)' % (_num(t[1]), n[t[2]], n[t[3]]))
+            elif t[0] == 'E2':
+                out.append('%s * hiz * (%s - rz * %s)' % (_num(t[1]), n[t[2]], n[t[3]]))
+            elif t[0] == 'EZH':
+                out.append('%s * hizh * %s' % (_num(t[1]), n[t[2]]))
+        return ' + '.join(out)
+
+    def emit(self, real='double'):
+        la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
+        L = self.L
+        na, nb, nc, nd = 2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1
+        nsph = na * nb * nc * nd
+        e_t, f_t = self.e_targets, self.f_targets
+        lines = []
+        w = lines.append
+        w('// class (%d %d | %d %d): %d VRR nodes, %d contracted accumulators, %d spherical outputs'
+          % (la, lb, lc, ld, len(self.vrr.order), len(e_t) * len(f_t), nsph))
+        w('template <> struct EriClass<%d, %d, %d, %d> {' % (la, lb, lc, ld))
+        w('    static constexpr int NSPH = %d;' % nsph)
+        w('    template <class BraT, class KetT>')
+        w('    __device__ __forceinline__ static void compute(const BraT& bra, const KetT& ket, const double* __restrict__ btab,')
+        w('                                                   double* __restrict__ out)')
+        w('    {')
+        for ie in range(len(e_t)):
+            for jf in range(len(f_t)):
+                w('        double c_%d_%d = 0.0;' % (ie, jf))
+        w('        const int kb = bra.nprim(), kk = ket.nprim();')
+        w('        for (int pb = 0; pb < kb; pb++) {')
+        w('            const double zeta = bra.zeta(pb), hiz = bra.hiz(pb), kab = bra.kfac(pb);')
+        w('            const double Px = bra.px(pb), Py = bra.py(pb), Pz = bra.pz(pb);')
+        w('            const double PBx = bra.pbx(pb), PBy = bra.pby(pb), PBz = bra.pbz(pb);')
+        w('            for (int pk = 0; pk < kk; pk++) {')
+        w('                const double eta = ket.zeta(pk), hie = ket.hiz(pk), kcd = ket.kfac(pk);')
+        w('                const double QDx = ket.pbx(pk), QDy = ket.pby(pk), QDz = ket.pbz(pk);')
+        w('                const double PQx = Px - ket.px(pk), PQy = Py - ket.py(pk), PQz = Pz - ket.pz(pk);')
+        w('                const double r = rsqrt(zeta + eta);')
+        w('                const double inv = r * r;')
+        w('                const double rz = eta * inv, rh = zeta * inv;')
+        w('                const double rho = zeta * rz;')
+        w('                const double hizh = 0.5 * inv;')
+        w('                const double WPx = -rz * PQx, WPy = -rz * PQy, WPz = -rz * PQz;')
+        w('                const double WQx = rh * PQx, WQy = rh * PQy, WQz = rh * PQz;')
+        w('                const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);')
+        w('                double F[%d];' % (L + 1))
+        w('                boys_function<%d>(T, F, btab);' % L)
+        w('                const double pref = kab * kcd * r;')
+        w('                #pragma unroll')
+        w('                for (int m = 0; m <= %d; m++) F[m] *= pref;' % L)
+        w('                (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;')
+        w('                (void)QDx; (void)QDy; (void)QDz; (void)PBx; (void)PBy; (void)PBz;')
+        w('                (void)hiz; (void)hie; (void)hizh; (void)rz; (void)rh;')
+        for key in self.vrr.order:
+            w('                const double %s = %s;' % (self.names[key], self._vrr_expr(key)))
+        for ie, e in enumerate(e_t):
+            for jf, f in enumerate(f_t):
+                w('                c_%d_%d += %s;' % (ie, jf, self.names[(e, f, 0)]))
+        w('            }')
+        w('        }')
+        # ---- ket HRR (per e target) then ket spherical
+        w('        const double DCx = ket.abx(), DCy = ket.aby(), DCz = ket.abz();')
+        w('        const double BAx = bra.abx(), BAy = bra.aby(), BAz = bra.abz();')
+        w('        (void)DCx; (void)DCy; (void)DCz; (void)BAx; (void)BAy; (void)BAz;')
+        f_index = {f: j for j, f in enumerate(f_t)}
+        ket_nodes, ket_order = {}, []
+
+        def need_ket(c, d):
+            key = (c, d)
+            if key in ket_nodes:
+                return key
+            if sum(c) == 0:
+                ket_nodes[key] = ('F', f_index[d])
+            else:
+                i = pick_axis(c)
+                c1 = sub1(c, i)
+                ket_nodes[key] = ('H', i, need_ket(c1, add1(d, i)), need_ket(c1, d))
+            ket_order.append(key)
+            return key
+
+        cc, dc = cart_list(lc), cart_list(ld)
+        for c in cc:
+            for d in dc:
+                need_ket(c, d)
+        sph_c, sph_d = sph_coefficients(lc), sph_coefficients(ld)
+        # half-transformed buffer h[ie][k][l]
+        for ie in range(len(e_t)):
+            names = {}
+            for n_, key in enumerate(ket_order):
+                node = ket_nodes[key]
+                nm = 'k%d_%d' % (ie, n_)
+                names[key] = nm
+                if node[0] == 'F':
+                    w('        const double %s = c_%d_%d;' % (nm, ie, node[1]))
+                else:
+                    w('        const double %s = %s + DC%s * %s;' % (nm, names[node[2]], AX[node[1]], names[node[3]]))
+            for k in range(nc):
+                for l in range(nd):
+                    terms = []
+                    for ic, c in enumerate(cc):
+                        if sph_c[k][ic] == 0.0:
+                            continue
+                        for jd, d in enumerate(dc):
+                            if sph_d[l][jd] == 0.0:
+                                continue
+                            terms.append('%s * %s' % (_num(sph_c[k][ic] * sph_d[l][jd]), names[(c, d)]))
+                    w('        const double h_%d_%d_%d = %s;' % (ie, k, l, ' + '.join(terms)))
+        # ---- bra HRR per (k, l), then bra spherical
+        e_index = {e: j for j, e in enumerate(e_t)}
+        bra_nodes, bra_order = {}, []
+
+        def need_bra(a, b):
+            key = (a, b)
+            if key in bra_nodes:
+                return key
+            if sum(a) == 0:
+                bra_nodes[key] = ('E', e_index[b])
+            else:
+                i = pick_axis(a)
+                a1 = sub1(a, i)
+                bra_nodes[key] = ('H', i, need_bra(a1, add1(b, i)), need_bra(a1, b))
+            bra_order.append(key)
+            return key
+
+        ac, bc = cart_list(la), cart_list(lb)
+        for a in ac:
+            for b in bc:
+                need_bra(a, b)
+        sph_a, sph_b = sph_coefficients(la), sph_coefficients(lb)
+        for k in range(nc):
+            for l in range(nd):
+                names = {}
+                for n_, key in enumerate(bra_order):
+                    node = bra_nodes[key]
+                    nm = 'b%d_%d_%d' % (k, l, n_)
+                    names[key] = nm
+                    if node[0] == 'E':
+                        w('        const double %s = h_%d_%d_%d;' % (nm, node[1], k, l))
+                    else:
+                        w('        const double %s = %s + BA%s * %s;' % (nm, names[node[2]], AX[node[1]], names[node[3]]))
+                for i in range(na):
+                    for j in range(nb):
+                        terms = []
+                        for ia, a in enumerate(ac):
+                            if sph_a[i][ia] == 0.0:
+                                continue
+                            for jb, b in enumerate(bc):
+                                if sph_b[j][jb] == 0.0:
+                                    continue
+                                terms.append('%s * %s' % (_num(sph_a[i][ia] * sph_b[j][jb]), names[(a, b)]))
+                        w('        out[%d] = %s;' % (((i * nb + j) * nc + k) * nd + l, ' + '.join(terms)))
+        w('    }')
+        w('};')
+        return '\n'.join(lines)
+
+
+    # --------------------------------------------------------- interpreter
+    def program(self):
+        """Recursion program for the table-driven kernel (vlx_interp.cu).
+
+        Slot 0 holds 0.0, slots 1..L+1 hold pref * F_m.  Ops (int4-quad + 2 doubles):
+          kind 0/1  VRR bra/ket: S[t] = G1*S[a] + G2*S[b] + c1*H*(S[c] - R*S[d]) + c2*hizh*S[e]
+          kind 2    accumulate:  S[t] += S[a]                       (per primitive quartet)
+          kind 3/4  HRR ket/bra: S[t] = S[a] + G*S[b]               (G = D - C or B - A)
+          kind 5    clear:       S[t] = 0
+          kind 6    axpy:        S[t] += c1 * S[a]
+        """
+        L = self.L
+        slot = {}
+        nxt = [L + 2]
+
+        def new():
+            s = nxt[0]
+            nxt[0] += 1
+            return s
+
+        vrr_ops = []
+        for key in self.vrr.order:
+            terms = self.vrr.nodes[key]
+            if terms[0][0] == 'BASE':
+                slot[key] = 1 + terms[0][1]
+                continue
+            t = new()
+            slot[key] = t
+            kind = 1 if terms[0][0] in ('QD', 'WQ') else 0
+            axis = terms[0][1]
+            a = slot[terms[0][2]]
+            b = slot[terms[1][2]]
+            c = d = e = 0
+            c1 = c2 = 0.0
+            for term in terms[2:]:
+                if term[0] in ('F2', 'E2'):
+                    c1 = float(term[1])
+                    c, d = slot[term[2]], slot[term[3]]
+                elif term[0] == 'EZH':
+                    c2 = float(term[1])
+                    e = slot[term[2]]
+            vrr_ops.append((kind * 4 + axis, t, a, b, c, d, e, c1, c2))
+        acc_slot = {}
+        acc_ops = []
+        for e in self.e_targets:
+            for f in self.f_targets:
+                s = new()
+                acc_slot[(e, f)] = s
+                acc_ops.append((2 * 4, s, slot[(e, f, 0)], 0, 0, 0, 0, 0.0, 0.0))
+        post = []
+        la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
+        nc_, nd_ = 2 * lc + 1, 2 * ld + 1
+        na_, nb_ = 2 * la + 1, 2 * lb + 1
+        cc, dc = cart_list(lc), cart_list(ld)
+        ac, bc = cart_list(la), cart_list(lb)
+        sph_c, sph_d = sph_coefficients(lc), sph_coefficients(ld)
+        sph_a, sph_b = sph_coefficients(la), sph_coefficients(lb)
+        # ket HRR per e target, then ket spherical -> h[e][k][l]
+        hslot = {}
+        for e in self.e_targets:
+            knodes = {}
+
+            def need_ket(c, d):
+                if (c, d) in knodes:
+                    return knodes[(c, d)]
+                if sum(c) == 0:
+                    knodes[(c, d)] = acc_slot[(e, d)]
+                else:
+                    i = pick_axis(c)
+                    c1_ = sub1(c, i)
+                    x = need_ket(c1_, add1(d, i))
+                    y = need_ket(c1_, d)
+                    t = new()
+                    post.append((3 * 4 + i, t, x, y, 0, 0, 0, 0.0, 0.0))
+                    knodes[(c, d)] = t
+                return knodes[(c, d)]
+
+            for c in cc:
+                for d in dc:
+                    need_ket(c, d)
+            for k in range(nc_):
+                for l in range(nd_):
+                    t = new()
+                    post.append((5 * 4, t, 0, 0, 0, 0, 0, 0.0, 0.0))
+                    for ic, c in enumerate(cc):
+                        for jd, d in enumerate(dc):
+                            cf = sph_c[k][ic] * sph_d[l][jd]
+                            if cf != 0.0:
+                                post.append((6 * 4, t, knodes[(c, d)], 0, 0, 0, 0, cf, 0.0))
+                    hslot[(e, k, l)] = t
+        out_slots = [0] * (na_ * nb_ * nc_ * nd_)
+        for k in range(nc_):
+            for l in range(nd_):
+                bnodes = {}
+
+                def need_bra(a, b):
+                    if (a, b) in bnodes:
+                        return bnodes[(a, b)]
+                    if sum(a) == 0:
+                        bnodes[(a, b)] = hslot[(b, k, l)]
+                    else:
+                        i = pick_axis(a)
+                        a1 = sub1(a, i)
+                        x = need_bra(a1, add1(b, i))
+                        y = need_bra(a1, b)
+                        t = new()
+                        post.append((4 * 4 + i, t, x, y, 0, 0, 0, 0.0, 0.0))
+                        bnodes[(a, b)] = t
+                    return bnodes[(a, b)]
+
+                for a in ac:
+                    for b in bc:
+                        need_bra(a, b)
+                for i in range(na_):
+                    for j in range(nb_):
+                        t = new()
+                        post.append((5 * 4, t, 0, 0, 0, 0, 0, 0.0, 0.0))
+                        for ia, a in enumerate(ac):
+                            for jb, b in enumerate(bc):
+                                cf = sph_a[i][ia] * sph_b[j][jb]
+                                if cf != 0.0:
+                                    post.append((6 * 4, t, bnodes[(a, b)], 0, 0, 0, 0, cf, 0.0))
+                        out_slots[((i * nb_ + j) * nc_ + k) * nd_ + l] = t
+        acc_first = min(acc_slot.values())
+        return dict(nslots=nxt[0], vrr=vrr_ops, acc=acc_ops, post=post, out=out_slots,
+                    acc_first=acc_first, nacc=len(acc_ops))
+
+def _num(v):
+    if isinstance(v, int):
+        return '%d.0' % v
+    if v == int(v) and abs(v) < 1e6:
+        return '%d.0' % int(v)
+    return repr(float(v))
+
+
+# ----------------------------------------------------------------- classes
+
+def pair_classes(lmax):
+    return [(a, b) for a in range(lmax + 1) for b in range(a, lmax + 1)]
+
+
+def pair_key(p):
+    return (p[0] + p[1], p[1])
+
+
+def quartet_classes(lmax):
+    """Canonical classes: bra pair key >= ket pair key (the bra carries more
+    angular momentum), each unordered pair of pair classes once."""
+    pcs = sorted(pair_classes(lmax), key=pair_key)
+    out = []
+    for i, k in enumerate(pcs):
+        for b in pcs[i:]:
+            out.append((b[0], b[1], k[0], k[1]))
+    return out
+
+
+def class_name(c):
+    return '%d%d%d%d' % c
+
+
+def emit_class_file(cls, outdir):
+    g = ClassGen(*cls)
+    la, lb, lc, ld = cls
+    nm = class_name(cls)
+    body = []
+    w = body.append
+    w('// Generated by gen_eri.py -- do not edit.')
+    w('#include "vlx_kernels.cuh"')
+    w('namespace vlx {')
+    w(g.emit())
+    w('')
+    w('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st)' % nm)
+    w('{')
+    w('    const dim3 blk(32 * kWarpsPerBlock);')
+    w('    quartet_kernel<%d, %d, %d, %d><<<grid, blk, 0, st>>>(a, mode);' % cls)
+    w('}')
+    w('int occupancy_quartet_%s(int mode)' % nm)
+    w('{')
+    w('    int n = 0;')
+    w('    (void)mode;')
+    w('    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel<%d, %d, %d, %d>, 32 * kWarpsPerBlock, 0);' % cls)
+    w('    return n;')
+    w('}')
+    if (la, lb) == (lc, ld):
+        w('void launch_schwarz_%d%d(const PairBlockDev* blocks, int bid, int npairs, const double* boys, double* maxv, cudaStream_t st)' % (la, lb))
+        w('{')
+        w('    if (npairs > 0) schwarz_kernel<%d, %d><<<(npairs + 63) / 64, 64, 0, st>>>(blocks, bid, boys, maxv);' % (la, lb))
+        w('}')
+    w('}  // namespace vlx')
+    text = '\n'.join(body) + '\n'
+    path = outdir / ('class_%s.cu' % nm)
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+    return path, g.stats()
+
+
+VRR_COMPILED_MAX = 2400
+
+
+def is_compiled(cls):
+    return len(ClassGen(*cls).vrr.order) <= VRR_COMPILED_MAX
+
+
+def emit_programs(classes, outdir):
+    """Recursion programs of the interpreted classes as one binary blob
+    (embedded into the library by vlx_blob.S, parsed by vlx_host.cu).
+
+    Layout (little-endian): int32 magic 0x564c5850, int32 count, then per class
+    14 int32 (la lb lc ld nvrr nacc_ops npost nslots acc_first nacc nout
+    op_offset out_offset pad), then all ops as int32[8] + float64[2] (48 bytes),
+    then all output slot lists as int32."""
+    import struct
+    heads, opbytes, outbytes = [], [], []
+    nops = nout = 0
+    for cls in classes:
+        p = ClassGen(*cls).program()
+        ops = p['vrr'] + p['acc'] + p['post']
+        heads.append(struct.pack('<14i', *cls, len(p['vrr']), len(p['acc']), len(p['post']), p['nslots'],
+                                 p['acc_first'], p['nacc'], len(p['out']), nops, nout, 0))
+        for op in ops:
+            opbytes.append(struct.pack('<8i2d', op[0], op[1], op[2], op[3], op[4], op[5], op[6], 0, op[7], op[8]))
+        outbytes.append(struct.pack('<%di' % len(p['out']), *p['out']))
+        nops += len(ops)
+        nout += len(p['out'])
+    blob = struct.pack('<2i', 0x564C5850, len(classes)) + b''.join(heads) + b''.join(opbytes) + b''.join(outbytes)
+    path = outdir / 'interp_programs.bin'
+    if not path.exists() or path.read_bytes() != blob:
+        path.write_bytes(blob)
+
+
+def emit_dispatch(compiled, lmax, outdir):
+    lines = ['// Generated by gen_eri.py -- do not edit.', '#pragma once', 'namespace vlx {']
+    for c in compiled:
+        nm = class_name(c)
+        lines.append('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st);' % nm)
+        lines.append('int occupancy_quartet_%s(int mode);' % nm)
+    schw = [(a, b) for (a, b) in pair_classes(lmax) if (a, b, a, b) in compiled]
+    for (a, b) in schw:
+        lines.append('void launch_schwarz_%d%d(const PairBlockDev* blocks, int bid, int npairs, const double* boys, double* maxv, cudaStream_t st);' % (a, b))
+    lines.append('struct QuartetClassEntry { int la, lb, lc, ld; void (*launch)(int, const FockArgs&, int, cudaStream_t); int (*occupancy)(int); };')
+    lines.append('static const QuartetClassEntry kQuartetClasses[] = {')
+    for c in compiled:
+        nm = class_name(c)
+        lines.append('    {%d, %d, %d, %d, launch_quartet_%s, occupancy_quartet_%s},' % (c + (nm, nm)))
+    lines.append('};')
+    lines.append('static const int kNumQuartetClasses = %d;' % len(compiled))
+    lines.append('struct SchwarzEntry { int la, lb; void (*launch)(const PairBlockDev*, int, int, const double*, double*, cudaStream_t); };')
+    lines.append('static const SchwarzEntry kSchwarzClasses[] = {')
+    for (a, b) in schw:
+        lines.append('    {%d, %d, launch_schwarz_%d%d},' % (a, b, a, b))
+    lines.append('};')
+    lines.append('static const int kNumSchwarzClasses = %d;' % len(schw))
+    lines.append('}  // namespace vlx')
+    text = '\n'.join(lines) + '\n'
+    path = outdir / 'dispatch.inc'
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+
+
+def main():
+    outdir = Path(sys.argv[1])
+    lmax = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+    outdir.mkdir(parents=True, exist_ok=True)
+    classes = quartet_classes(lmax)
+    compiled = [c for c in classes if is_compiled(c)]
+    interp = [c for c in classes if not is_compiled(c)]
+    for cls in compiled:
+        emit_class_file(cls, outdir)
+    emit_dispatch(compiled, lmax, outdir)
+    emit_programs(interp, outdir)
+    for p in outdir.glob('class_*.cu'):
+        if tuple(int(ch) for ch in p.stem[6:]) not in compiled:
+            p.unlink()
+    print('compiled classes:', len(compiled), 'interpreted classes:', len(interp))
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,959 @@
+// Host orchestration of the B200 Fock build and the C ABI of include/vlx_b200.h.
+//
+//  * shells, GTO blocks (l, nprim) and pair blocks in the reference order
+//    (src/orbdata/GtoFunc.cpp:9-18, GtoPairBlockFunc.cpp:16-43,
+//    GtoPairBlock.cpp:49-305);
+//  * per-pair primitive data as SoA device arrays [field][prim][pair];
+//  * Schwarz diagonals on the GPU, decade bins as in
+//    src/orbdata/BlockedGtoPairBlock.cpp:22-42, pairs re-sorted by bin so the
+//    kets admitted for a bra of bin b are a prefix of the ket block;
+//  * work items (bra pair x run of ket pairs) per quartet class, the selection
+//    rule of src/general/OpenMPFunc.cpp:121-259 (bin_bra + bin_ket <= ithreshold,
+//    each unordered pair of pairs once), dealt round-robin over ranks like
+//    omp::partition_tasks (src/general/OpenMPFunc.hpp:89-112);
+//  * one persistent launch per quartet class with a work-queue head, then
+//    F = acc + acc^T for symmetric densities (src/math/Matrix.cpp:189-197).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vlx_b200.h"
+#include "vlx_interp.cuh"
+#include "vlx_kernels.cuh"
+#include "dispatch.inc"
+
+extern "C" const char vlx_interp_blob_start[];
+extern "C" const char vlx_interp_blob_end[];
+
+using vlx::FockArgs;
+using vlx::InterpClassDev;
+using vlx::PairBlockDev;
+using vlx::WorkItem;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define VLX_CUDA(x)                                                                                  \
+    do {                                                                                             \
+        cudaError_t e_ = (x);                                                                        \
+        if (e_ != cudaSuccess) return fail(VLX_B200_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------ basis
+// CBasisFunction::normalize / _rescale / _overlap (BasisFunction.cpp:129-260)
+double lnorm(int l)
+{
+    static const double f[7] = {1.0, 2.0, 1.1547005383792515, 1.0327955589886444, 0.19518001458970663,
+                                0.13012000972647107, 0.039235786222290345};
+    return f[l];
+}
+
+void normalize_shell(int l, int n, const double* e, double* c)
+{
+    if (n == 1) c[0] = 1.0;
+    for (int i = 0; i < n; i++) {
+        c[i] *= std::pow(e[i] * 2.0 / M_PI, 0.75);
+        c[i] *= lnorm(l) * std::pow(e[i], 0.5 * l);
+    }
+    static const double lfac[7] = {1.0, 0.5, 3.0, 7.5, 420.0, 1890.0, 41580.0};
+    double s = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) {
+            const double fab = 1.0 / (e[i] + e[j]);
+            double fovl = M_PI * fab;
+            fovl = c[i] * c[j] * fovl * std::sqrt(fovl);
+            if (i != j) fovl *= 2.0;
+            s += (l == 0 ? 1.0 : lfac[l] * std::pow(fab, l)) * fovl;
+        }
+    s = 1.0 / std::sqrt(s);
+    for (int i = 0; i < n; i++) c[i] *= s;
+}
+
+// ------------------------------------------------------------------ Boys table
+// F_m(T) = e^{-T} sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)), long double.
+long double boys_series(int m, long double t)
+{
+    long double term = 1.0L / (2 * m + 1), sum = term;
+    for (int k = 1; k < 1000; k++) {
+        term *= 2.0L * t / (2 * m + 2 * k + 1);
+        sum += term;
+        if (term < 1e-24L * sum) break;
+    }
+    return std::exp(-t) * sum;
+}
+
+std::vector<double> make_boys_table()
+{
+    const int N = BOYS_NCOEF;
+    std::vector<double> tab((size_t)(BOYS_MMAX + 1) * BOYS_NINT * N);
+    for (int m = 0; m <= BOYS_MMAX; m++)
+        for (int it = 0; it < BOYS_NINT; it++) {
+            long double fv[BOYS_NCOEF];
+            for (int k = 0; k < N; k++) {
+                const long double x = std::cos(M_PI * (k + 0.5L) / N);
+                fv[k] = boys_series(m, it + 0.5L + 0.5L * x);
+            }
+            for (int j = 0; j < N; j++) {
+                long double s = 0.0L;
+                for (int k = 0; k < N; k++) s += fv[k] * std::cos(M_PI * j * (k + 0.5L) / N);
+                s *= 2.0L / N;
+                if (j == 0) s *= 0.5L;
+                tab[((size_t)(m * BOYS_NINT + it)) * N + j] = (double)s;
+            }
+        }
+    return tab;
+}
+
+// ------------------------------------------------------------------ per-device globals
+struct DeviceGlobals {
+    bool ready = false;
+    int nsm = 0;
+    double* boys = nullptr;
+    void* prog = nullptr;
+    std::vector<InterpClassDev> interp;
+};
+
+std::mutex g_dev_mutex;
+std::map<int, DeviceGlobals> g_dev;
+
+int device_globals(int device, DeviceGlobals** out)
+{
+    std::lock_guard<std::mutex> lock(g_dev_mutex);
+    DeviceGlobals& g = g_dev[device];
+    if (!g.ready) {
+        VLX_CUDA(cudaSetDevice(device));
+        VLX_CUDA(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, device));
+        const auto tab = make_boys_table();
+        VLX_CUDA(cudaMalloc(&g.boys, tab.size() * sizeof(double)));
+        VLX_CUDA(cudaMemcpy(g.boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        // interpreter programs: int32 header, per class 14 int32, ops (8 int32 + 2 double), outs
+        const char* blob = vlx_interp_blob_start;
+        const size_t bsize = (size_t)(vlx_interp_blob_end - vlx_interp_blob_start);
+        int head[2];
+        std::memcpy(head, blob, sizeof(head));
+        if (head[0] != 0x564C5850) return fail(VLX_B200_ERR_CUDA, "corrupt interpreter program blob");
+        const int ncls = head[1];
+        std::vector<int> ch((size_t)ncls * 14);
+        std::memcpy(ch.data(), blob + 8, ch.size() * sizeof(int));
+        size_t nops = 0, nout = 0;
+        for (int c = 0; c < ncls; c++) {
+            nops += ch[c * 14 + 4] + ch[c * 14 + 5] + ch[c * 14 + 6];
+            nout += ch[c * 14 + 10];
+        }
+        const char* ops = blob + 8 + ch.size() * sizeof(int);
+        const char* outs = ops + nops * 48;
+        if ((size_t)(outs + nout * 4 - blob) > bsize) return fail(VLX_B200_ERR_CUDA, "truncated program blob");
+        std::vector<int> opi(nops * 8);
+        std::vector<double> opd(nops * 2);
+        for (size_t o = 0; o < nops; o++) {
+            std::memcpy(&opi[o * 8], ops + o * 48, 32);
+            std::memcpy(&opd[o * 2], ops + o * 48 + 32, 16);
+        }
+        const size_t bytes_i = opi.size() * 4, bytes_d = opd.size() * 8, bytes_o = nout * 4;
+        char* dev = nullptr;
+        VLX_CUDA(cudaMalloc(&dev, bytes_i + bytes_d + bytes_o + 64));
+        VLX_CUDA(cudaMemcpy(dev, opi.data(), bytes_i, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMemcpy(dev + bytes_i, opd.data(), bytes_d, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMemcpy(dev + bytes_i + bytes_d, outs, bytes_o, cudaMemcpyHostToDevice));
+        g.prog = dev;
+        for (int c = 0; c < ncls; c++) {
+            const int* h = &ch[c * 14];
+            InterpClassDev d;
+            d.la = h[0];
+            d.lb = h[1];
+            d.lc = h[2];
+            d.ld = h[3];
+            d.nvrr = h[4];
+            d.nacc_ops = h[5];
+            d.npost = h[6];
+            d.nslots = h[7];
+            d.acc_first = h[8];
+            d.nacc = h[9];
+            d.nout = h[10];
+            d.opi = reinterpret_cast<const int4*>(dev) + (size_t)h[11] * 2;
+            d.opd = reinterpret_cast<const double2*>(dev + bytes_i) + h[11];
+            d.out = reinterpret_cast<const int*>(dev + bytes_i + bytes_d) + h[12];
+            g.interp.push_back(d);
+        }
+        g.ready = true;
+    }
+    *out = &g;
+    return VLX_B200_OK;
+}
+
+// ------------------------------------------------------------------ kernels local to the host TU
+__global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ out, const int n)
+{
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x;
+    for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+        const int r = bx * 32 + ty, c = by * 32 + tx;
+        tile[ty][tx] = (r < n && c < n) ? acc[(size_t)r * n + c] : 0.0;
+    }
+    __syncthreads();
+    for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+        const int i = by * 32 + ty, j = bx * 32 + tx;
+        if (i < n && j < n) out[(size_t)i * n + j] = acc[(size_t)i * n + j] + tile[tx][ty];
+    }
+}
+
+template <int M>
+__global__ void boys_test_kernel(const double* T, double* F, int n, const double* tab)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double f[M + 1];
+    vlx::boys_function<M>(T[i], f, tab);
+    F[i] = f[M];
+}
+
+template <int M>
+void launch_boys_test(int m, const double* T, double* F, int n, const double* tab)
+{
+    if (m == M)
+        boys_test_kernel<M><<<(n + 127) / 128, 128>>>(T, F, n, tab);
+    else if constexpr (M > 0)
+        launch_boys_test<M - 1>(m, T, F, n, tab);
+}
+
+// ------------------------------------------------------------------ screener state
+struct Shell {
+    double xyz[3];
+    int l, nprim, ao0;
+    std::vector<double> e, c;
+};
+
+struct PairBlock {
+    int la, lb, ka, kb;
+    std::vector<std::pair<int, int>> pairs;  // reference order
+    std::vector<double> maxv;                // reference order
+    std::vector<int> bin;                    // reference order
+    std::vector<int> sorted;                 // sorted position -> reference index (bins >= 0)
+    int bin_off[17];                         // sorted pairs with bin < b start at bin_off[b]
+};
+
+struct ClassTasks {
+    int compiled = -1;  // index into kQuartetClasses
+    int interp = -1;    // index into DeviceGlobals::interp
+    std::vector<WorkItem> items;
+    size_t offset = 0;
+};
+
+struct TaskSet {
+    int ith = 0, rank = 0, nodes = 1, seg = 0;
+    std::vector<ClassTasks> classes;
+    WorkItem* d_items = nullptr;
+    long long quartets = 0, prim_quartets = 0;
+};
+
+int pair_key(int la, int lb) { return (la + lb) * 16 + lb; }
+
+}  // namespace
+
+struct vlx_b200_screener {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DeviceGlobals* glob = nullptr;
+    int nao = 0, lmax = 0;
+    int nl[VLX_LMAX + 1] = {0};
+    std::vector<Shell> shells;
+    std::vector<PairBlock> blocks;
+    std::vector<PairBlockDev> h_blocks;
+    PairBlockDev* d_blocks = nullptr;
+    char* d_pairs = nullptr;
+    double* d_D = nullptr;
+    double* d_F = nullptr;
+    double* d_acc = nullptr;
+    int* d_counters = nullptr;
+    int ncounters = 0;
+    double* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int seg = 256;
+    std::vector<TaskSet> tasksets;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+// Builds device arrays of all pair blocks; `sorted` selects the screened,
+// bin-sorted pair order instead of the reference order.
+int upload_pairs(vlx_b200_screener* s, bool sorted)
+{
+    const size_t nb = s->blocks.size();
+    std::vector<size_t> offs(nb + 1, 0);
+    std::vector<int> npairs(nb);
+    for (size_t b = 0; b < nb; b++) {
+        const PairBlock& pb = s->blocks[b];
+        const size_t n = sorted ? pb.sorted.size() : pb.pairs.size();
+        npairs[b] = (int)n;
+        const size_t k = (size_t)pb.ka * pb.kb;
+        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + 2 * n * sizeof(int);
+        bytes = (bytes + 255) & ~size_t(255);
+        offs[b + 1] = offs[b] + bytes;
+    }
+    std::vector<char> host(offs[nb] + 256, 0);
+    s->h_blocks.assign(nb, PairBlockDev{});
+    const double kconst = std::sqrt(2.0 / std::sqrt(M_PI));
+    for (size_t b = 0; b < nb; b++) {
+        const PairBlock& pb = s->blocks[b];
+        const size_t n = npairs[b];
+        const int kp = pb.ka * pb.kb;
+        double* prim = reinterpret_cast<double*>(host.data() + offs[b]);
+        double* ab = prim + 9 * (size_t)kp * n;
+        int* ao = reinterpret_cast<int*>(ab + 3 * n);
+        for (size_t i = 0; i < n; i++) {
+            const int ref = sorted ? pb.sorted[i] : (int)i;
+            const Shell& A = s->shells[pb.pairs[ref].first];
+            const Shell& B = s->shells[pb.pairs[ref].second];
+            double r2 = 0.0;
+            for (int x = 0; x < 3; x++) {
+                ab[x * n + i] = B.xyz[x] - A.xyz[x];
+                r2 += (B.xyz[x] - A.xyz[x]) * (B.xyz[x] - A.xyz[x]);
+            }
+            ao[i] = A.ao0;
+            ao[n + i] = B.ao0;
+            for (int ka = 0; ka < pb.ka; ka++)
+                for (int kb = 0; kb < pb.kb; kb++) {
+                    const int p = ka * pb.kb + kb;
+                    const double ea = A.e[ka], eb = B.e[kb], z = ea + eb;
+                    const double fz = M_PI / z;
+                    const double sab = fz * std::sqrt(fz) * std::exp(-ea * eb / z * r2);
+                    const double cab = A.c[ka] * B.c[kb] * sab;
+                    double v[9];
+                    v[0] = z;
+                    v[1] = 0.5 / z;
+                    v[2] = cab * std::sqrt(z) * kconst;
+                    for (int x = 0; x < 3; x++) {
+                        v[3 + x] = (ea * A.xyz[x] + eb * B.xyz[x]) / z;
+                        v[6 + x] = v[3 + x] - B.xyz[x];
+                    }
+                    for (int f = 0; f < 9; f++) prim[((size_t)f * kp + p) * n + i] = v[f];
+                }
+        }
+    }
+    if (s->d_pairs) cudaFree(s->d_pairs);
+    s->d_pairs = nullptr;
+    VLX_CUDA(cudaMalloc(&s->d_pairs, host.size()));
+    VLX_CUDA(cudaMemcpy(s->d_pairs, host.data(), host.size(), cudaMemcpyHostToDevice));
+    for (size_t b = 0; b < nb; b++) {
+        const PairBlock& pb = s->blocks[b];
+        const size_t n = npairs[b];
+        const int kp = pb.ka * pb.kb;
+        PairBlockDev d;
+        d.prim = reinterpret_cast<const double*>(s->d_pairs + offs[b]);
+        d.ab = d.prim + 9 * (size_t)kp * n;
+        d.ao = reinterpret_cast<const int*>(d.ab + 3 * n);
+        d.npairs = (int)n;
+        d.kprim = kp;
+        d.la = pb.la;
+        d.lb = pb.lb;
+        s->h_blocks[b] = d;
+    }
+    if (!s->d_blocks) VLX_CUDA(cudaMalloc(&s->d_blocks, std::max<size_t>(1, nb) * sizeof(PairBlockDev)));
+    VLX_CUDA(cudaMemcpy(s->d_blocks, s->h_blocks.data(), nb * sizeof(PairBlockDev), cudaMemcpyHostToDevice));
+    return VLX_B200_OK;
+}
+
+int find_compiled(int la, int lb, int lc, int ld)
+{
+    for (int c = 0; c < vlx::kNumQuartetClasses; c++) {
+        const auto& e = vlx::kQuartetClasses[c];
+        if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return c;
+    }
+    return -1;
+}
+
+int find_interp(const DeviceGlobals* g, int la, int lb, int lc, int ld)
+{
+    for (size_t c = 0; c < g->interp.size(); c++) {
+        const auto& e = g->interp[c];
+        if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return (int)c;
+    }
+    return -1;
+}
+
+// Scratch of the table-driven kernel: nslots doubles per resident thread,
+// capped at 2 GiB (the grid shrinks instead).
+int interp_grid(vlx_b200_screener* s, const InterpClassDev& c, int threads_per_block, int want_blocks, int* grid)
+{
+    const size_t per_thread = (size_t)c.nslots * sizeof(double);
+    const size_t cap = size_t(2) << 30;
+    int blocks = std::min(want_blocks, s->glob->nsm * 4);
+    while (blocks > 1 && per_thread * blocks * threads_per_block > cap) blocks--;
+    blocks = std::max(blocks, 1);
+    const size_t need = per_thread * blocks * threads_per_block;
+    if (need > s->scratch_bytes) {
+        if (s->d_scratch) cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        VLX_CUDA(cudaMalloc(&s->d_scratch, need));
+        s->scratch_bytes = need;
+    }
+    *grid = blocks;
+    return VLX_B200_OK;
+}
+
+int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
+{
+    const size_t nb = s->blocks.size();
+    std::vector<double*> d_max(nb, nullptr);
+    for (size_t b = 0; b < nb; b++) {
+        const PairBlock& pb = s->blocks[b];
+        const int n = (int)pb.pairs.size();
+        VLX_CUDA(cudaMalloc(&d_max[b], std::max(1, n) * sizeof(double)));
+        bool done = false;
+        for (int c = 0; c < vlx::kNumSchwarzClasses; c++) {
+            if (vlx::kSchwarzClasses[c].la == pb.la && vlx::kSchwarzClasses[c].lb == pb.lb) {
+                vlx::kSchwarzClasses[c].launch(s->d_blocks, (int)b, n, s->glob->boys, d_max[b], s->stream);
+                done = true;
+            }
+        }
+        if (!done) {
+            const int ic = find_interp(s->glob, pb.la, pb.lb, pb.la, pb.lb);
+            if (ic < 0) return fail(VLX_B200_ERR_UNSUPPORTED, "no kernel for Schwarz class");
+            int grid = 0;
+            const int want = (n + 63) / 64;
+            int rc = interp_grid(s, s->glob->interp[ic], 64, std::max(1, want), &grid);
+            if (rc) return rc;
+            vlx::launch_interp_schwarz(s->d_blocks, (int)b, s->glob->interp[ic], s->glob->boys, s->d_scratch, grid,
+                                       d_max[b], s->stream);
+        }
+        VLX_CUDA(cudaGetLastError());
+    }
+    VLX_CUDA(cudaStreamSynchronize(s->stream));
+    maxv.assign(nb, {});
+    for (size_t b = 0; b < nb; b++) {
+        maxv[b].resize(s->blocks[b].pairs.size());
+        if (!maxv[b].empty())
+            VLX_CUDA(cudaMemcpy(maxv[b].data(), d_max[b], maxv[b].size() * sizeof(double), cudaMemcpyDeviceToHost));
+        cudaFree(d_max[b]);
+    }
+    return VLX_B200_OK;
+}
+
+int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** out)
+{
+    for (auto& t : s->tasksets)
+        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg) {
+            *out = &t;
+            return VLX_B200_OK;
+        }
+    TaskSet ts;
+    ts.ith = ith;
+    ts.rank = rank;
+    ts.nodes = nodes;
+    ts.seg = s->seg;
+    std::map<int, int> cls_index;  // key -> position in ts.classes
+    long long g = 0;
+    const size_t nb = s->blocks.size();
+    for (size_t qi = 0; qi < nb; qi++)
+        for (size_t qj = qi; qj < nb; qj++) {
+            const PairBlock& A = s->blocks[qi];
+            const PairBlock& B = s->blocks[qj];
+            if (A.sorted.empty() || B.sorted.empty()) continue;
+            size_t bra = qi, ket = qj;
+            if (pair_key(A.la, A.lb) < pair_key(B.la, B.lb)) std::swap(bra, ket);
+            const PairBlock& Pb = s->blocks[bra];
+            const PairBlock& Pk = s->blocks[ket];
+            const int key = ((Pb.la * 8 + Pb.lb) * 8 + Pk.la) * 8 + Pk.lb;
+            auto it = cls_index.find(key);
+            if (it == cls_index.end()) {
+                ClassTasks ct;
+                ct.compiled = find_compiled(Pb.la, Pb.lb, Pk.la, Pk.lb);
+                if (ct.compiled < 0) ct.interp = find_interp(s->glob, Pb.la, Pb.lb, Pk.la, Pk.lb);
+                if (ct.compiled < 0 && ct.interp < 0)
+                    return fail(VLX_B200_ERR_UNSUPPORTED, "quartet class not compiled in");
+                it = cls_index.emplace(key, (int)ts.classes.size()).first;
+                ts.classes.push_back(ct);
+            }
+            ClassTasks& ct = ts.classes[it->second];
+            const bool diag = (qi == qj);
+            const int nbra = (int)Pb.sorted.size();
+            const long long kp = (long long)Pb.ka * Pb.kb * Pk.ka * Pk.kb;
+            for (int x = 0; x < nbra; x++) {
+                const int bx = Pb.bin[Pb.sorted[x]];
+                const int kmax = ith - bx;
+                if (kmax < 0) break;
+                const int kend = Pk.bin_off[std::min(kmax, 15) + 1];
+                const int kbeg = diag ? x : 0;
+                for (int k0 = kbeg; k0 < kend; k0 += s->seg) {
+                    const int k1 = std::min(kend, k0 + s->seg);
+                    if ((g++ % nodes) != rank) continue;
+                    WorkItem w;
+                    w.blocks = (int)bra | ((int)ket << 16);
+                    w.bra = x;
+                    w.kbeg = k0;
+                    w.kend = k1;
+                    ct.items.push_back(w);
+                    ts.quartets += k1 - k0;
+                    ts.prim_quartets += (long long)(k1 - k0) * kp;
+                }
+            }
+        }
+    size_t total = 0;
+    for (auto& ct : ts.classes) {
+        ct.offset = total;
+        total += ct.items.size();
+    }
+    if (total > 0) {
+        std::vector<WorkItem> all;
+        all.reserve(total);
+        for (auto& ct : ts.classes) all.insert(all.end(), ct.items.begin(), ct.items.end());
+        VLX_CUDA(cudaMalloc(&ts.d_items, total * sizeof(WorkItem)));
+        VLX_CUDA(cudaMemcpy(ts.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    }
+    if ((int)ts.classes.size() > s->ncounters) {
+        if (s->d_counters) cudaFree(s->d_counters);
+        s->ncounters = std::max<int>(64, (int)ts.classes.size());
+        VLX_CUDA(cudaMalloc(&s->d_counters, s->ncounters * sizeof(int)));
+    }
+    // keep the cache small: the SCF changes ithreshold only a few times
+    if (s->tasksets.size() >= 8) {
+        if (s->tasksets.front().d_items) cudaFree(s->tasksets.front().d_items);
+        s->tasksets.erase(s->tasksets.begin());
+    }
+    s->tasksets.push_back(std::move(ts));
+    *out = &s->tasksets.back();
+    return VLX_B200_OK;
+}
+
+bool label_weights(const char* label, int symmetric, double xfac, double* cj, double* ck)
+{
+    const std::string l(label ? label : "");
+    const double j = symmetric ? 2.0 : 1.0;
+    if (l == "2jk") { *cj = 2.0 * j; *ck = -1.0; return true; }
+    if (l == "2jkx") { *cj = 2.0 * j; *ck = -xfac; return true; }
+    if (l == "j" || l == "j_rs") { *cj = j; *ck = 0.0; return true; }
+    if (l == "k" || l == "k_rs") { *cj = 0.0; *ck = 1.0; return true; }
+    if (l == "kx" || l == "kx_rs") { *cj = 0.0; *ck = xfac; return true; }
+    *cj = 0.0;
+    *ck = 0.0;
+    return false;
+}
+
+int ensure_buffers(vlx_b200_screener* s)
+{
+    const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    if (!s->d_acc) VLX_CUDA(cudaMalloc(&s->d_acc, std::max<size_t>(bytes, 8)));
+    if (!s->d_D) VLX_CUDA(cudaMalloc(&s->d_D, std::max<size_t>(bytes, 8)));
+    if (!s->d_F) VLX_CUDA(cudaMalloc(&s->d_F, std::max<size_t>(bytes, 8)));
+    return VLX_B200_OK;
+}
+
+// Enqueues all class kernels of a task set on `st`; F (accumulator) must be zeroed.
+int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
+                    double cj, double ck, cudaStream_t st, long long* launches)
+{
+    if (ts->classes.empty()) return VLX_B200_OK;
+    VLX_CUDA(cudaMemsetAsync(s->d_counters, 0, ts->classes.size() * sizeof(int), st));
+    FockArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.blocks = s->d_blocks;
+    a.boys = s->glob->boys;
+    a.D = dD;
+    a.F = dAcc;
+    a.eri = eri;
+    a.nao = s->nao;
+    for (int l = 0; l <= VLX_LMAX; l++) a.nl[l] = s->nl[l];
+    a.cj = cj;
+    a.ck = ck;
+    const int warps_per_block = vlx::kWarpsPerBlock;
+    for (size_t c = 0; c < ts->classes.size(); c++) {
+        ClassTasks& ct = ts->classes[c];
+        if (ct.items.empty()) continue;
+        a.items = ts->d_items + ct.offset;
+        a.nitems = (int)ct.items.size();
+        a.counter = s->d_counters + c;
+        const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
+        if (ct.compiled >= 0) {
+            const auto& e = vlx::kQuartetClasses[ct.compiled];
+            const int occ = std::max(1, e.occupancy(mode));
+            const int grid = std::max(1, std::min(want, occ * s->glob->nsm));
+            e.launch(mode, a, grid, st);
+        } else {
+            int grid = 0;
+            int rc = interp_grid(s, s->glob->interp[ct.interp], 128, std::max(1, want), &grid);
+            if (rc) return rc;
+            vlx::launch_interp_quartet(mode, a, s->glob->interp[ct.interp], s->d_scratch, grid, st);
+        }
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    }
+    return VLX_B200_OK;
+}
+
+int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, int symmetric, const char* label,
+                 double xfac, double omega, int ith, double* dF, cudaStream_t st, long long* quartets,
+                 long long* prim, long long* launches)
+{
+    if (omega != 0.0) return fail(VLX_B200_ERR_UNSUPPORTED, "range-separated (omega != 0) integrals not compiled in");
+    if (nodes < 1 || rank < 0 || rank >= nodes) return fail(VLX_B200_ERR_ARGUMENT, "invalid rank / nodes");
+    double cj = 0.0, ck = 0.0;
+    const bool known = label_weights(label, symmetric, xfac, &cj, &ck);
+    int rc = ensure_buffers(s);
+    if (rc) return rc;
+    const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
+    if (known) {
+        TaskSet* ts = nullptr;
+        rc = build_tasks(s, ith, rank, nodes, &ts);
+        if (rc) return rc;
+        rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dD, s->d_acc, nullptr, cj,
+                             ck, st, launches);
+        if (rc) return rc;
+        if (quartets) *quartets += ts->quartets;
+        if (prim) *prim += ts->prim_quartets;
+    }
+    if (symmetric) {
+        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, dF, s->nao);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    } else {
+        VLX_CUDA(cudaMemcpyAsync(dF, s->d_acc, bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    return VLX_B200_OK;
+}
+
+int host_build(vlx_b200_screener* s, int rank, int nodes, const double* density, int symmetric, const char* label,
+               double xfac, double omega, int ith, double* fock_out, vlx_b200_stats* stats)
+{
+    if (!s || !density || !fock_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    VLX_CUDA(cudaSetDevice(s->device));
+    int rc = ensure_buffers(s);
+    if (rc) return rc;
+    const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    VLX_CUDA(cudaMemcpyAsync(s->d_D, density, bytes, cudaMemcpyHostToDevice, s->stream));
+    long long q = 0, pq = 0, nl = 0;
+    VLX_CUDA(cudaEventRecord(s->ev0, s->stream));
+    rc = device_build(s, rank, nodes, s->d_D, symmetric, label, xfac, omega, ith, s->d_F, s->stream, &q, &pq, &nl);
+    if (rc) return rc;
+    VLX_CUDA(cudaEventRecord(s->ev1, s->stream));
+    VLX_CUDA(cudaMemcpyAsync(fock_out, s->d_F, bytes, cudaMemcpyDeviceToHost, s->stream));
+    VLX_CUDA(cudaStreamSynchronize(s->stream));
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        stats->device_ms = ms;
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->shell_quartets = q;
+        stats->prim_quartets = pq;
+        stats->kernel_launches = nl;
+    }
+    return VLX_B200_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+const char* vlx_b200_version(void) { return "vlx_b200 0.1 (sm_100a, FP64 HGP, L<=3)"; }
+
+const char* vlx_b200_last_error(void) { return g_err.c_str(); }
+
+int vlx_b200_device_count(int* count)
+{
+    if (!count) return fail(VLX_B200_ERR_ARGUMENT, "null count");
+    *count = 0;
+    const cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        *count = 0;
+        cudaGetLastError();
+        return fail(VLX_B200_ERR_NO_DEVICE, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    }
+    return VLX_B200_OK;
+}
+
+int vlx_b200_normalize_shell(int l, int nprim, const double* exponents, double* coefficients)
+{
+    if (l < 0 || l > 6 || nprim < 1 || !exponents || !coefficients)
+        return fail(VLX_B200_ERR_ARGUMENT, "normalize_shell: invalid arguments");
+    normalize_shell(l, nprim, exponents, coefficients);
+    return VLX_B200_OK;
+}
+
+int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, const double* xyz, int nshells,
+                             const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                             const double* exponents, const double* coefficients)
+{
+    if (!out || natoms < 1 || nshells < 1 || !xyz || !shell_atom || !shell_l || !shell_nprim || !exponents ||
+        !coefficients)
+        return fail(VLX_B200_ERR_ARGUMENT, "screener_create: invalid arguments");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(VLX_B200_ERR_NO_DEVICE, "screener_create: no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(VLX_B200_ERR_ARGUMENT, "screener_create: bad device index");
+    for (int i = 0; i < nshells; i++) {
+        if (shell_l[i] < 0 || shell_nprim[i] < 1 || shell_atom[i] < 0 || shell_atom[i] >= natoms)
+            return fail(VLX_B200_ERR_ARGUMENT, "screener_create: invalid shell table");
+        if (shell_l[i] > VLX_LMAX)
+            return fail(VLX_B200_ERR_UNSUPPORTED, "screener_create: angular momentum above f is not compiled in");
+    }
+    auto s = new vlx_b200_screener();
+    s->device = device;
+    int rc = 0;
+    auto cleanup = [&](int code) {
+        vlx_b200_screener_destroy(s);
+        return code;
+    };
+    rc = device_globals(device, &s->glob);
+    if (rc) return cleanup(rc);
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) ||
+        cudaEventCreate(&s->ev0) || cudaEventCreate(&s->ev1))
+        return cleanup(fail(VLX_B200_ERR_CUDA, "screener_create: stream / event creation failed"));
+    // shells and the AO map (MolecularBasis.cpp:468-490)
+    size_t off = 0;
+    s->shells.resize(nshells);
+    for (int i = 0; i < nshells; i++) {
+        Shell& sh = s->shells[i];
+        sh.l = shell_l[i];
+        sh.nprim = shell_nprim[i];
+        for (int x = 0; x < 3; x++) sh.xyz[x] = xyz[3 * shell_atom[i] + x];
+        sh.e.assign(exponents + off, exponents + off + sh.nprim);
+        sh.c.assign(coefficients + off, coefficients + off + sh.nprim);
+        off += sh.nprim;
+        normalize_shell(sh.l, sh.nprim, sh.e.data(), sh.c.data());
+        s->lmax = std::max(s->lmax, sh.l);
+    }
+    int loff[VLX_LMAX + 2] = {0}, cnt[VLX_LMAX + 1] = {0};
+    for (auto& sh : s->shells) s->nl[sh.l]++;
+    for (int l = 0; l <= VLX_LMAX; l++) loff[l + 1] = loff[l] + s->nl[l] * (2 * l + 1);
+    s->nao = loff[VLX_LMAX + 1];
+    for (auto& sh : s->shells) sh.ao0 = loff[sh.l] + cnt[sh.l]++;
+    // GTO blocks (l ascending, distinct contraction depths ascending)
+    std::vector<std::pair<int, int>> gblocks;  // (l, K)
+    std::vector<std::vector<int>> gshells;
+    for (int l = 0; l <= s->lmax; l++) {
+        std::vector<int> ks;
+        for (auto& sh : s->shells)
+            if (sh.l == l) ks.push_back(sh.nprim);
+        std::sort(ks.begin(), ks.end());
+        ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
+        for (int k : ks) {
+            gblocks.push_back({l, k});
+            std::vector<int> members;
+            for (int i = 0; i < nshells; i++)
+                if (s->shells[i].l == l && s->shells[i].nprim == k) members.push_back(i);
+            gshells.push_back(members);
+        }
+    }
+    const int ng = (int)gblocks.size();
+    if (ng * (ng + 1) / 2 > 0xffff) return cleanup(fail(VLX_B200_ERR_UNSUPPORTED, "too many pair blocks"));
+    for (int i = 0; i < ng; i++)
+        for (int j = i; j < ng; j++) {
+            PairBlock pb;
+            pb.la = gblocks[i].first;
+            pb.ka = gblocks[i].second;
+            pb.lb = gblocks[j].first;
+            pb.kb = gblocks[j].second;
+            const auto& A = gshells[i];
+            const auto& B = gshells[j];
+            if (i == j) {
+                for (size_t y = 0; y < A.size(); y++)
+                    for (size_t x = 0; x <= y; x++) pb.pairs.push_back({A[x], A[y]});
+            } else {
+                for (int x : A)
+                    for (int y : B) pb.pairs.push_back({x, y});
+            }
+            s->blocks.push_back(std::move(pb));
+        }
+    // Schwarz diagonals on the device, in reference pair order
+    rc = upload_pairs(s, false);
+    if (rc) return cleanup(rc);
+    std::vector<std::vector<double>> maxv;
+    rc = run_schwarz(s, maxv);
+    if (rc) return cleanup(rc);
+    for (size_t b = 0; b < s->blocks.size(); b++) {
+        PairBlock& pb = s->blocks[b];
+        pb.maxv = maxv[b];
+        pb.bin.resize(pb.maxv.size());
+        int count[16] = {0};
+        for (size_t i = 0; i < pb.maxv.size(); i++) {
+            const double fct = std::sqrt(pb.maxv[i]);
+            pb.bin[i] = (fct > 1.0e-15) ? ((fct < 1.0) ? int(-std::floor(std::log10(fct))) : 0) : -1;
+            if (pb.bin[i] >= 0) count[pb.bin[i]]++;
+        }
+        pb.bin_off[0] = 0;
+        for (int k = 0; k < 16; k++) pb.bin_off[k + 1] = pb.bin_off[k] + count[k];
+        pb.sorted.clear();
+        for (int k = 0; k < 16; k++)
+            for (size_t i = 0; i < pb.bin.size(); i++)
+                if (pb.bin[i] == k) pb.sorted.push_back((int)i);
+    }
+    rc = upload_pairs(s, true);
+    if (rc) return cleanup(rc);
+    *out = s;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_screener_destroy(vlx_b200_screener* s)
+{
+    if (!s) return VLX_B200_OK;
+    cudaSetDevice(s->device);
+    for (auto& t : s->tasksets)
+        if (t.d_items) cudaFree(t.d_items);
+    if (s->d_pairs) cudaFree(s->d_pairs);
+    if (s->d_blocks) cudaFree(s->d_blocks);
+    if (s->d_D) cudaFree(s->d_D);
+    if (s->d_F) cudaFree(s->d_F);
+    if (s->d_acc) cudaFree(s->d_acc);
+    if (s->d_counters) cudaFree(s->d_counters);
+    if (s->d_scratch) cudaFree(s->d_scratch);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_screener_nao(const vlx_b200_screener* s, int* nao)
+{
+    if (!s || !nao) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    *nao = s->nao;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_screener_npairs(const vlx_b200_screener* s, int* npairs)
+{
+    if (!s || !npairs) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    size_t n = 0;
+    for (auto& b : s->blocks) n += b.pairs.size();
+    *npairs = (int)n;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_screener_pair_info(const vlx_b200_screener* s, int* info, double* maxv)
+{
+    if (!s || !info || !maxv) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    size_t k = 0;
+    for (size_t b = 0; b < s->blocks.size(); b++) {
+        const PairBlock& pb = s->blocks[b];
+        for (size_t i = 0; i < pb.pairs.size(); i++, k++) {
+            info[6 * k + 0] = (int)b;
+            info[6 * k + 1] = pb.bin[i];
+            info[6 * k + 2] = pb.la;
+            info[6 * k + 3] = pb.lb;
+            info[6 * k + 4] = s->shells[pb.pairs[i].first].ao0;
+            info[6 * k + 5] = s->shells[pb.pairs[i].second].ao0;
+            maxv[k] = pb.maxv[i];
+        }
+    }
+    return VLX_B200_OK;
+}
+
+int vlx_b200_set_block_size_factor(vlx_b200_screener* s, int factor)
+{
+    if (!s || factor < 1) return fail(VLX_B200_ERR_ARGUMENT, "invalid block size factor");
+    s->seg = std::max(32, (256 / factor) / 32 * 32);
+    return VLX_B200_OK;
+}
+
+int vlx_b200_fock_build(vlx_b200_screener* s, const double* density, int symmetric, const char* label,
+                        double xfac, double omega, int ith, double* fock_out, vlx_b200_stats* stats)
+{
+    return host_build(s, 0, 1, density, symmetric, label, xfac, omega, ith, fock_out, stats);
+}
+
+int vlx_b200_fock_build_local(vlx_b200_screener* s, int rank, int nodes, const double* density, int symmetric,
+                              const char* label, double xfac, double omega, int ith, double* fock_out,
+                              vlx_b200_stats* stats)
+{
+    return host_build(s, rank, nodes, density, symmetric, label, xfac, omega, ith, fock_out, stats);
+}
+
+int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int ndens, const double* const* densities,
+                              int symmetric, const char* const* labels, double xfac, double omega, int ith,
+                              double* const* focks_out, vlx_b200_stats* stats)
+{
+    if (!s || ndens < 1 || !densities || !labels || !focks_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    vlx_b200_stats acc{};
+    for (int i = 0; i < ndens; i++) {
+        vlx_b200_stats one{};
+        const int rc = host_build(s, rank, nodes, densities[i], symmetric, labels[i], xfac, omega, ith, focks_out[i],
+                                  &one);
+        if (rc) return rc;
+        acc.device_ms += one.device_ms;
+        acc.total_ms += one.total_ms;
+        acc.shell_quartets += one.shell_quartets;
+        acc.prim_quartets += one.prim_quartets;
+        acc.kernel_launches += one.kernel_launches;
+    }
+    if (stats) *stats = acc;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_fock_build_device(vlx_b200_screener* s, const double* d_density, int symmetric, const char* label,
+                               double xfac, double omega, int ith, double* d_fock, void* stream)
+{
+    if (!s || !d_density || !d_fock) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    VLX_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    return device_build(s, 0, 1, d_density, symmetric, label, xfac, omega, ith, d_fock, st, nullptr, nullptr, nullptr);
+}
+
+int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
+{
+    if (!s || !eri_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    VLX_CUDA(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->nao;
+    const size_t bytes = n * n * n * n * sizeof(double);
+    double* d_eri = nullptr;
+    VLX_CUDA(cudaMalloc(&d_eri, bytes));
+    int rc = VLX_B200_OK;
+    TaskSet* ts = nullptr;
+    cudaError_t e = cudaMemsetAsync(d_eri, 0, bytes, s->stream);
+    if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    if (!rc) rc = ensure_buffers(s);
+    if (!rc) rc = build_tasks(s, ith, 0, 1, &ts);
+    if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, s->stream, nullptr);
+    if (!rc) {
+        e = cudaMemcpyAsync(eri_out, d_eri, bytes, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(d_eri);
+    return rc;
+}
+
+int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F)
+{
+    if (m < 0 || m > BOYS_MMAX || n < 1 || !T || !F) return fail(VLX_B200_ERR_ARGUMENT, "boys_device: bad args");
+    DeviceGlobals* g = nullptr;
+    int rc = device_globals(device, &g);
+    if (rc) return rc;
+    VLX_CUDA(cudaSetDevice(device));
+    double *dT = nullptr, *dF = nullptr;
+    VLX_CUDA(cudaMalloc(&dT, n * sizeof(double)));
+    VLX_CUDA(cudaMalloc(&dF, n * sizeof(double)));
+    cudaMemcpy(dT, T, n * sizeof(double), cudaMemcpyHostToDevice);
+    launch_boys_test<BOYS_MMAX>(m, dT, dF, n, g->boys);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(F, dF, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dT);
+    cudaFree(dF);
+    if (e != cudaSuccess) return fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    return VLX_B200_OK;
+}
+
+}  // extern "C"

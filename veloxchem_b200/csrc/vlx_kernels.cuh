@@ -1,0 +1,254 @@
+// Kernel templates instantiated once per quartet class by the generated
+// translation units (gen_eri.py).  One warp owns one work item: a bra shell
+// pair (warp-uniform) against a run of ket shell pairs, one ket pair per lane.
+// Work items are pulled from a per-launch queue head with atomicAdd, so the
+// grid is persistent (sized to the resident capacity of the SMs).
+#pragma once
+
+#include "vlx_device.cuh"
+
+namespace vlx {
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double ldD(const double* __restrict__ D, int nao, int r, int c)
+{
+    return __ldg(D + (size_t)r * nao + c);
+}
+
+__device__ __forceinline__ void addF(double* F, int nao, int r, int c, double v)
+{
+    atomicAdd(F + (size_t)r * nao + c, v);
+}
+
+// J/K digestion of the spherical block f[((i NB + j) NC + k) ND + l] of one
+// unique shell quartet (P Q | R S).  s carries the permutational weight
+// (1/2 for P == Q, 1/2 for R == S, 1/2 for PQ == RS) and is 0 on idle lanes.
+// Symmetric density (reference local_distribute_rest_*): contributions are
+// accumulated in one orientation and the caller adds the transpose at the end.
+template <int NA, int NB, int NC, int ND, int MODE>
+__device__ __forceinline__ void digest(const double* f, const double s, const int lane, const int p0, const int nlp,
+                                       const int q0, const int nlq, const int r0, const int nlr, const int s0,
+                                       const int nls, const FockArgs& a)
+{
+    const double* __restrict__ D = a.D;
+    double* F = a.F;
+    const int nao = a.nao;
+    const double cj = a.cj * s, ck = a.ck * s;
+    if (a.cj != 0.0) {
+        // F_PQ: reduce over the lanes (ket pairs), then one atomic per element
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+#pragma unroll
+                    for (int l = 0; l < ND; l++) {
+                        double d = ldD(D, nao, r0 + k * nlr, s0 + l * nls);
+                        if (MODE == MODE_FOCK_GEN) d += ldD(D, nao, s0 + l * nls, r0 + k * nlr);
+                        v = fma(f[((i * NB + j) * NC + k) * ND + l], d, v);
+                    }
+                }
+                v = warp_sum(v * cj);
+                if (lane == ((i * NB + j) & 31)) {
+                    addF(F, nao, p0 + i * nlp, q0 + j * nlq, v);
+                    if (MODE == MODE_FOCK_GEN) addF(F, nao, q0 + j * nlq, p0 + i * nlp, v);
+                }
+            }
+        }
+        // F_RS: per lane
+        if (s != 0.0) {
+#pragma unroll
+            for (int k = 0; k < NC; k++) {
+#pragma unroll
+                for (int l = 0; l < ND; l++) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NA; i++) {
+#pragma unroll
+                        for (int j = 0; j < NB; j++) {
+                            double d = ldD(D, nao, p0 + i * nlp, q0 + j * nlq);
+                            if (MODE == MODE_FOCK_GEN) d += ldD(D, nao, q0 + j * nlq, p0 + i * nlp);
+                            v = fma(f[((i * NB + j) * NC + k) * ND + l], d, v);
+                        }
+                    }
+                    addF(F, nao, r0 + k * nlr, s0 + l * nls, cj * v);
+                    if (MODE == MODE_FOCK_GEN) addF(F, nao, s0 + l * nls, r0 + k * nlr, cj * v);
+                }
+            }
+        }
+    }
+    if (a.ck != 0.0 && s != 0.0) {
+        // F_PR += sum_{j l} f D_QS ; F_RP (general) += sum f D_SQ
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+#pragma unroll
+            for (int k = 0; k < NC; k++) {
+                double v = 0.0, w = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+#pragma unroll
+                    for (int l = 0; l < ND; l++) {
+                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        v = fma(x, ldD(D, nao, q0 + j * nlq, s0 + l * nls), v);
+                        if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, s0 + l * nls, q0 + j * nlq), w);
+                    }
+                }
+                addF(F, nao, p0 + i * nlp, r0 + k * nlr, ck * v);
+                if (MODE == MODE_FOCK_GEN) addF(F, nao, r0 + k * nlr, p0 + i * nlp, ck * w);
+            }
+        }
+        // F_PS += sum_{j k} f D_QR
+#pragma unroll
+        for (int i = 0; i < NA; i++) {
+#pragma unroll
+            for (int l = 0; l < ND; l++) {
+                double v = 0.0, w = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        v = fma(x, ldD(D, nao, q0 + j * nlq, r0 + k * nlr), v);
+                        if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, r0 + k * nlr, q0 + j * nlq), w);
+                    }
+                }
+                addF(F, nao, p0 + i * nlp, s0 + l * nls, ck * v);
+                if (MODE == MODE_FOCK_GEN) addF(F, nao, s0 + l * nls, p0 + i * nlp, ck * w);
+            }
+        }
+        // F_QR += sum_{i l} f D_PS
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+#pragma unroll
+            for (int k = 0; k < NC; k++) {
+                double v = 0.0, w = 0.0;
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+#pragma unroll
+                    for (int l = 0; l < ND; l++) {
+                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        v = fma(x, ldD(D, nao, p0 + i * nlp, s0 + l * nls), v);
+                        if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, s0 + l * nls, p0 + i * nlp), w);
+                    }
+                }
+                addF(F, nao, q0 + j * nlq, r0 + k * nlr, ck * v);
+                if (MODE == MODE_FOCK_GEN) addF(F, nao, r0 + k * nlr, q0 + j * nlq, ck * w);
+            }
+        }
+        // F_QS += sum_{i k} f D_PR
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+#pragma unroll
+            for (int l = 0; l < ND; l++) {
+                double v = 0.0, w = 0.0;
+#pragma unroll
+                for (int i = 0; i < NA; i++) {
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        v = fma(x, ldD(D, nao, p0 + i * nlp, r0 + k * nlr), v);
+                        if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, r0 + k * nlr, p0 + i * nlp), w);
+                    }
+                }
+                addF(F, nao, q0 + j * nlq, s0 + l * nls, ck * v);
+                if (MODE == MODE_FOCK_GEN) addF(F, nao, s0 + l * nls, q0 + j * nlq, ck * w);
+            }
+        }
+    }
+}
+
+// Scatter one unique spherical quartet into the dense ERI tensor (all eight
+// index permutations), as CT4CEriTensorDistributor does.
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void scatter_eri(const double* f, const int p0, const int nlp, const int q0, const int nlq,
+                                            const int r0, const int nlr, const int s0, const int nls, double* eri,
+                                            const int nao)
+{
+    const size_t n = (size_t)nao;
+    for (int i = 0; i < NA; i++)
+        for (int j = 0; j < NB; j++)
+            for (int k = 0; k < NC; k++)
+                for (int l = 0; l < ND; l++) {
+                    const size_t p = p0 + i * nlp, q = q0 + j * nlq, r = r0 + k * nlr, t = s0 + l * nls;
+                    const double v = f[((i * NB + j) * NC + k) * ND + l];
+                    eri[((p * n + q) * n + r) * n + t] = v;
+                    eri[((q * n + p) * n + r) * n + t] = v;
+                    eri[((p * n + q) * n + t) * n + r] = v;
+                    eri[((q * n + p) * n + t) * n + r] = v;
+                    eri[((r * n + t) * n + p) * n + q] = v;
+                    eri[((t * n + r) * n + p) * n + q] = v;
+                    eri[((r * n + t) * n + q) * n + p] = v;
+                    eri[((t * n + r) * n + q) * n + p] = v;
+                }
+}
+
+constexpr int kWarpsPerBlock = 4;
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const FockArgs a, const int mode)
+{
+    using C = EriClass<LA, LB, LC, LD>;
+    constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
+    const int lane = threadIdx.x & 31;
+    const int nlp = a.nl[LA], nlq = a.nl[LB], nlr = a.nl[LC], nls = a.nl[LD];
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(a.counter, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= a.nitems) return;
+        const WorkItem w = a.items[it];
+        const int bbi = w.blocks & 0xffff, kbi = w.blocks >> 16;
+        const PairBlockDev bb = a.blocks[bbi];
+        const PairBlockDev kb = a.blocks[kbi];
+        const PairView bra = make_view(bb, w.bra);
+        const int p0 = __ldg(bb.ao + w.bra), q0 = __ldg(bb.ao + bb.npairs + w.bra);
+        const double s_bra = (p0 == q0) ? 0.5 : 1.0;
+        for (int j0 = w.kbeg; j0 < w.kend; j0 += 32) {
+            const int j = j0 + lane;
+            const bool act = j < w.kend;
+            const int jj = act ? j : (w.kend - 1);
+            const PairView ket = make_view(kb, jj);
+            double f[C::NSPH];
+            C::compute(bra, ket, a.boys, f);
+            const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
+            if (mode == MODE_ERI) {
+                if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, a.nao);
+            } else {
+                double s = act ? s_bra : 0.0;
+                if (r0 == s0) s *= 0.5;
+                if (bbi == kbi && jj == w.bra) s *= 0.5;
+                if (mode == MODE_FOCK_SYM)
+                    digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);
+                else
+                    digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);
+            }
+        }
+    }
+}
+
+// max over all spherical components of (ab|ab) per pair (T4CScreener::partition)
+template <int LA, int LB>
+__global__ void __launch_bounds__(64) schwarz_kernel(const PairBlockDev* blocks, const int bid, const double* boys,
+                                                     double* maxv)
+{
+    using C = EriClass<LA, LB, LA, LB>;
+    const PairBlockDev b = blocks[bid];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b.npairs) return;
+    const PairView v = make_view(b, i);
+    double f[C::NSPH];
+    C::compute(v, v, boys, f);
+    double mx = 0.0;
+    for (int t = 0; t < C::NSPH; t++) mx = (f[t] > mx) ? f[t] : mx;
+    maxv[i] = mx;
+}
+
+}  // namespace vlx

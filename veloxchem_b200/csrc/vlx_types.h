@@ -1,0 +1,53 @@
+// Types shared by the host orchestration (vlx_host.cu) and the device kernels.
+#pragma once
+
+#include <stdint.h>
+
+// Boys-function Chebyshev table: orders 0..BOYS_MMAX, unit intervals on
+// [0, BOYS_TMAX), BOYS_NCOEF coefficients per (order, interval).
+#define BOYS_MMAX 16
+#define BOYS_TMAX 40
+#define BOYS_NINT 40
+#define BOYS_NCOEF 14
+
+// Highest angular momentum per shell compiled into the class kernels.
+#define VLX_LMAX 3
+
+namespace vlx {
+
+// One pair block (shell pairs of GTO blocks (la, Ka) x (lb, Kb)), pairs sorted
+// by Schwarz bin.  Arrays live in one device allocation owned by the screener.
+struct PairBlockDev {
+    const double* prim;  // [9][kprim][npairs]
+    const double* ab;    // [3][npairs]  B - A
+    const int* ao;       // [2][npairs]  AO index of component 0 of A and of B
+    int npairs;
+    int kprim;
+    int la, lb;
+};
+
+// A run of ket pairs for one bra pair of one (bra block, ket block) job.
+struct WorkItem {
+    int blocks;  // bra block | (ket block << 16)
+    int bra;     // bra pair index within its block
+    int kbeg;    // ket pair range [kbeg, kend) within the ket block
+    int kend;
+};
+
+enum KernelMode { MODE_FOCK_SYM = 0, MODE_FOCK_GEN = 1, MODE_ERI = 2 };
+
+struct FockArgs {
+    const PairBlockDev* blocks;
+    const WorkItem* items;
+    int nitems;
+    int* counter;             // work-queue head for this launch (zeroed before)
+    const double* boys;       // Chebyshev table
+    const double* D;          // density, nao x nao row-major
+    double* F;                // accumulator, nao x nao row-major
+    double* eri;              // MODE_ERI: nao^4 tensor
+    int nao;
+    int nl[VLX_LMAX + 1];     // shells per angular momentum (AO stride of component m)
+    double cj, ck;            // J and K weights of the label
+};
+
+}  // namespace vlx
