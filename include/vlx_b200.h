@@ -130,6 +130,29 @@ int vlx_b200_compute_eri(vlx_b200_screener* screener, int ithreshold, double* er
  * (host arrays T[n] in, F[n] out), for validation. */
 int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F);
 
+/* Per-class record of a profiled build. */
+typedef struct {
+    int la, lb, lc, ld;        /* quartet class (bra la <= lb | ket lc <= ld) */
+    int table_driven;          /* 1 if served by the table-driven kernel */
+    double device_ms;          /* CUDA-event duration of the class launch */
+    long long shell_quartets;  /* unique shell quartets in the launch */
+    long long prim_quartets;   /* primitive quartets in the launch */
+    double flops;              /* algorithmic FP64 flops of the launch */
+} vlx_b200_class_profile;
+
+/* A device-resident build (as vlx_b200_fock_build_device, ithreshold and
+ * label as there, omega = 0) with one CUDA-event pair around each quartet-class
+ * launch on `stream`; synchronises and fills up to max_classes records.
+ * Measurement entry point, no counterpart in the reference. */
+int vlx_b200_fock_profile(vlx_b200_screener* screener, const double* d_density, int symmetric, const char* label,
+                          double exchange_factor, int ithreshold, double* d_fock, void* stream, int max_classes,
+                          vlx_b200_class_profile* out, int* nclasses);
+
+/* Measured FP64 FMA throughput of `device` (TFLOP/s, best of 5 launches of an
+ * FMA-chain probe kernel): the roofline denominator of the FP64 recursions.
+ * Measurement entry point, no counterpart in the reference. */
+int vlx_b200_fp64_peak(int device, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,7 +13,7 @@ from conftest import ROOT, load_golden
 
 def declared_symbols():
     text = (ROOT / 'include' / 'vlx_b200.h').read_text()
-    return sorted(set(re.findall(r'\b(vlx_b200_[a-z_]+)\s*\(', text)))
+    return sorted(set(re.findall(r'\b(vlx_b200_[a-z0-9_]+)\s*\(', text)))
 
 
 def test_library_exports_every_declared_symbol():

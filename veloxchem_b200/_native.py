@@ -41,7 +41,37 @@ SIGNATURES = {
                                                   ctypes.c_double, ctypes.c_int, _vp, _vp]),
     'vlx_b200_compute_eri': (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     'vlx_b200_boys_device': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    'vlx_b200_fock_profile': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double, ctypes.c_int,
+                                             _vp, _vp, ctypes.c_int, _vp, _ip]),
+    'vlx_b200_fp64_peak': (ctypes.c_int, [ctypes.c_int, _dp]),
 }
+
+
+class ClassProfile(ctypes.Structure):
+    _fields_ = [('la', ctypes.c_int), ('lb', ctypes.c_int), ('lc', ctypes.c_int), ('ld', ctypes.c_int),
+                ('table_driven', ctypes.c_int), ('device_ms', ctypes.c_double),
+                ('shell_quartets', ctypes.c_longlong), ('prim_quartets', ctypes.c_longlong),
+                ('flops', ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def fp64_peak(device=0):
+    v = ctypes.c_double(0.0)
+    check(lib().vlx_b200_fp64_peak(int(device), ctypes.byref(v)), 'fp64_peak')
+    return v.value
+
+
+def fock_profile(screener, d_density_ptr, d_fock_ptr, label='2jk', xfac=1.0, ithreshold=12, symmetric=True,
+                 stream_ptr=None, max_classes=256):
+    arr = (ClassProfile * max_classes)()
+    n = ctypes.c_int(0)
+    check(lib().vlx_b200_fock_profile(screener.handle, ctypes.c_void_p(d_density_ptr), int(symmetric),
+                                      label.encode(), float(xfac), int(ithreshold), ctypes.c_void_p(d_fock_ptr),
+                                      ctypes.c_void_p(stream_ptr) if stream_ptr else None, max_classes,
+                                      ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(n)), 'fock_profile')
+    return [arr[i].as_dict() for i in range(n.value)]
 
 
 class Stats(ctypes.Structure):

@@ -2,7 +2,7 @@
 
 Steps: generate the per-class recursions (csrc/gen_eri.py) into csrc/_gen,
 compile every translation unit with nvcc in parallel (incremental: a unit is
-rebuilt when its source or any shared header changed), embed the interpreter
+rebuilt when its source or any shared header changed), embed the warp-cooperative
 program blob, link one shared library with the static CUDA runtime.
 
     python -m veloxchem_b200.build [--jobs N] [--lmax 3]
@@ -66,15 +66,15 @@ def build(jobs=None, lmax=3, verbose=True):
     import gen_eri
     sys.argv = ['gen_eri.py', str(GEN), str(lmax)]
     gen_eri.main()
-    blob = GEN / 'interp_programs.bin'
+    blob = GEN / 'coop_programs.bin'
     asm = GEN / 'vlx_blob.S'
-    asm_text = ('    .section .rodata\n    .global vlx_interp_blob_start\n    .global vlx_interp_blob_end\n'
-                '    .balign 16\nvlx_interp_blob_start:\n    .incbin "%s"\nvlx_interp_blob_end:\n'
+    asm_text = ('    .section .rodata\n    .global vlx_coop_blob_start\n    .global vlx_coop_blob_end\n'
+                '    .balign 16\nvlx_coop_blob_start:\n    .incbin "%s"\nvlx_coop_blob_end:\n'
                 '    .byte 0\n    .section .note.GNU-stack,"",@progbits\n' % blob)
     if not asm.exists() or asm.read_text() != asm_text:
         asm.write_text(asm_text)
     hdr = _headers_digest()
-    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_interp.cu', CSRC / 'vlx_host.cu']
+    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_host.cu']
     objs = [OBJ / (s.stem + '.o') for s in sources]
     jobs = jobs or os.cpu_count() or 4
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -89,7 +89,7 @@ def build(jobs=None, lmax=3, verbose=True):
     if not blob_obj.exists() or not blob_stamp.exists() or blob_stamp.read_text() != blob_key:
         subprocess.run(['gcc', '-c', str(asm), '-o', str(blob_obj)], check=True)
         blob_stamp.write_text(blob_key)
-    # stale class objects (classes that moved to the interpreter) are not linked
+    # only the objects of the current class list are linked
     link = [nvcc()] + ARCH + ['-shared', '-o', str(LIB)] + [str(o) for o in objs] + [str(blob_obj)]
     res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:

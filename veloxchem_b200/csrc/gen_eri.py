@@ -210,14 +210,16 @@ class ClassGen:
             for jf in range(len(f_t)):
                 w('        double c_%d_%d = 0.0;' % (ie, jf))
         w('        const int kb = bra.nprim(), kk = ket.nprim();')
-        w('        for (int pb = 0; pb < kb; pb++) {')
-        w('            const double zeta = bra.zeta(pb), hiz = bra.hiz(pb), kab = bra.kfac(pb);')
-        w('            const double Px = bra.px(pb), Py = bra.py(pb), Pz = bra.pz(pb);')
-        w('            const double PBx = bra.pbx(pb), PBy = bra.pby(pb), PBz = bra.pbz(pb);')
-        w('            for (int pk = 0; pk < kk; pk++) {')
-        w('                const double eta = ket.zeta(pk), hie = ket.hiz(pk), kcd = ket.kfac(pk);')
-        w('                const double QDx = ket.pbx(pk), QDy = ket.pby(pk), QDz = ket.pbz(pk);')
-        w('                const double PQx = Px - ket.px(pk), PQy = Py - ket.py(pk), PQz = Pz - ket.pz(pk);')
+        # ket primitives outer: the ket data is per lane (loaded once per ket
+        # primitive), the bra data is warp-uniform (broadcast loads)
+        w('        for (int pk = 0; pk < kk; pk++) {')
+        w('            const double eta = ket.zeta(pk), hie = ket.hiz(pk), kcd = ket.kfac(pk);')
+        w('            const double QDx = ket.pbx(pk), QDy = ket.pby(pk), QDz = ket.pbz(pk);')
+        w('            const double Qx = ket.px(pk), Qy = ket.py(pk), Qz = ket.pz(pk);')
+        w('            for (int pb = 0; pb < kb; pb++) {')
+        w('                const double zeta = bra.zeta(pb), hiz = bra.hiz(pb), kab = bra.kfac(pb);')
+        w('                const double PBx = bra.pbx(pb), PBy = bra.pby(pb), PBz = bra.pbz(pb);')
+        w('                const double PQx = bra.px(pb) - Qx, PQy = bra.py(pb) - Qy, PQz = bra.pz(pb) - Qz;')
         w('                const double r = rsqrt(zeta + eta);')
         w('                const double inv = r * r;')
         w('                const double rz = eta * inv, rh = zeta * inv;')
@@ -337,9 +339,34 @@ class ClassGen:
         return '\n'.join(lines)
 
 
+
+    # --------------------------------------------------------- flop counts
+    def flops(self):
+        """Algorithmic FP64 operation counts of the recursion (1 per add or
+        multiply): per primitive quartet the VRR graph (node-for-node the
+        reference's ElectronRepulsionPrimRec* graph) plus one add per
+        contracted accumulator; per contracted quartet the HRR nodes (2 each)
+        and the spherical transforms (2 per nonzero factor)."""
+        vrr = 0
+        for key in self.vrr.order:
+            terms = self.vrr.nodes[key]
+            if terms[0][0] == 'BASE':
+                continue
+            for n_, t in enumerate(terms):
+                cost = {'QD': 1, 'WQ': 1, 'PB': 1, 'WP': 1, 'F2': 4, 'E2': 4, 'EZH': 2}[t[0]]
+                vrr += cost + (1 if n_ > 0 else 0)
+        acc = len(self.e_targets) * len(self.f_targets)
+        p = self.program()
+        post = 0
+        for op in p['post']:
+            kind = op[0] >> 2
+            if kind in (3, 4, 6):
+                post += 2
+        return vrr, acc, post
+
     # --------------------------------------------------------- interpreter
     def program(self):
-        """Recursion program for the table-driven kernel (vlx_interp.cu).
+        """Linear recursion program of the class (used for the operation counts).
 
         Slot 0 holds 0.0, slots 1..L+1 hold pref * F_m.  Ops (int4-quad + 2 doubles):
           kind 0/1  VRR bra/ket: S[t] = G1*S[a] + G2*S[b] + c1*H*(S[c] - R*S[d]) + c2*hizh*S[e]
@@ -534,37 +561,14 @@ def emit_class_file(cls, outdir):
 
 
 VRR_COMPILED_MAX = 2400
+ACC_COMPILED_MAX = 180
 
 
 def is_compiled(cls):
-    return len(ClassGen(*cls).vrr.order) <= VRR_COMPILED_MAX
-
-
-def emit_programs(classes, outdir):
-    """Recursion programs of the interpreted classes as one binary blob
-    (embedded into the library by vlx_blob.S, parsed by vlx_host.cu).
-
-    Layout (little-endian): int32 magic 0x564c5850, int32 count, then per class
-    14 int32 (la lb lc ld nvrr nacc_ops npost nslots acc_first nacc nout
-    op_offset out_offset pad), then all ops as int32[8] + float64[2] (48 bytes),
-    then all output slot lists as int32."""
-    import struct
-    heads, opbytes, outbytes = [], [], []
-    nops = nout = 0
-    for cls in classes:
-        p = ClassGen(*cls).program()
-        ops = p['vrr'] + p['acc'] + p['post']
-        heads.append(struct.pack('<14i', *cls, len(p['vrr']), len(p['acc']), len(p['post']), p['nslots'],
-                                 p['acc_first'], p['nacc'], len(p['out']), nops, nout, 0))
-        for op in ops:
-            opbytes.append(struct.pack('<8i2d', op[0], op[1], op[2], op[3], op[4], op[5], op[6], 0, op[7], op[8]))
-        outbytes.append(struct.pack('<%di' % len(p['out']), *p['out']))
-        nops += len(ops)
-        nout += len(p['out'])
-    blob = struct.pack('<2i', 0x564C5850, len(classes)) + b''.join(heads) + b''.join(opbytes) + b''.join(outbytes)
-    path = outdir / 'interp_programs.bin'
-    if not path.exists() or path.read_bytes() != blob:
-        path.write_bytes(blob)
+    """Straight-line register kernel when the contracted buffer and the
+    recursion graph are small enough; otherwise the warp-cooperative kernel."""
+    g = ClassGen(*cls)
+    return len(g.vrr.order) <= VRR_COMPILED_MAX and len(g.e_targets) * len(g.f_targets) <= ACC_COMPILED_MAX
 
 
 def emit_dispatch(compiled, lmax, outdir):
@@ -576,11 +580,12 @@ def emit_dispatch(compiled, lmax, outdir):
     schw = [(a, b) for (a, b) in pair_classes(lmax) if (a, b, a, b) in compiled]
     for (a, b) in schw:
         lines.append('void launch_schwarz_%d%d(const PairBlockDev* blocks, int bid, int npairs, const double* boys, double* maxv, cudaStream_t st);' % (a, b))
-    lines.append('struct QuartetClassEntry { int la, lb, lc, ld; void (*launch)(int, const FockArgs&, int, cudaStream_t); int (*occupancy)(int); };')
+    lines.append('struct QuartetClassEntry { int la, lb, lc, ld; void (*launch)(int, const FockArgs&, int, cudaStream_t); int (*occupancy)(int); int prim_flops, post_flops; };')
     lines.append('static const QuartetClassEntry kQuartetClasses[] = {')
     for c in compiled:
         nm = class_name(c)
-        lines.append('    {%d, %d, %d, %d, launch_quartet_%s, occupancy_quartet_%s},' % (c + (nm, nm)))
+        fv, fa, fp = ClassGen(*c).flops()
+        lines.append('    {%d, %d, %d, %d, launch_quartet_%s, occupancy_quartet_%s, %d, %d},' % (c + (nm, nm, fv + fa, fp)))
     lines.append('};')
     lines.append('static const int kNumQuartetClasses = %d;' % len(compiled))
     lines.append('struct SchwarzEntry { int la, lb; void (*launch)(const PairBlockDev*, int, int, const double*, double*, cudaStream_t); };')
@@ -603,14 +608,18 @@ def main():
     classes = quartet_classes(lmax)
     compiled = [c for c in classes if is_compiled(c)]
     interp = [c for c in classes if not is_compiled(c)]
+    for p in ('interp_programs.bin',):
+        if (outdir / p).exists():
+            (outdir / p).unlink()
     for cls in compiled:
         emit_class_file(cls, outdir)
     emit_dispatch(compiled, lmax, outdir)
-    emit_programs(interp, outdir)
+    import gen_coop
+    gen_coop.emit_blob(interp, outdir / 'coop_programs.bin')
     for p in outdir.glob('class_*.cu'):
         if tuple(int(ch) for ch in p.stem[6:]) not in compiled:
             p.unlink()
-    print('compiled classes:', len(compiled), 'interpreted classes:', len(interp))
+    print('compiled classes:', len(compiled), 'warp-cooperative classes:', len(interp))
 
 
 if __name__ == '__main__':

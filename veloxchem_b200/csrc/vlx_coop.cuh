@@ -1,0 +1,27 @@
+// Interface of the warp-cooperative quartet kernel (vlx_coop.cu).
+#pragma once
+
+#include "vlx_device.cuh"
+
+namespace vlx {
+
+// One class program (pointers into the device copy of the program blob).
+struct CoopClassDev {
+    int la, lb, lc, ld;
+    int nslots, nacc, nbody, npost, nblev, nplev;
+    const int4* opi;     // 2 x int4 per op: {kind*4+axis, dst, x, y}, {u, v, w, c1 | c2 << 8}
+    const double2* opw;  // 2 x double2 per op: {w0, w1}, {w2, 0}
+    const int* boff;     // body level offsets (index l = first op of level l; levels 1..nblev)
+    const int* poff;     // post level offsets
+    const int* fslots;   // slot of pref * F_m, m = 0..la+lb+lc+ld (0 = unused)
+    const int* outs;     // slot of spherical component ((i NB + j) NC + k) ND + l
+};
+
+cudaError_t coop_prepare();
+int coop_blocks_per_sm(const CoopClassDev& c);
+int coop_warps_per_block(const CoopClassDev& c);
+void launch_coop_quartet(int mode, const FockArgs& a, const CoopClassDev& c, int grid, cudaStream_t st);
+void launch_coop_schwarz(const PairBlockDev* blocks, int bid, int npairs, const CoopClassDev& c, const double* boys,
+                         double* maxv, int nsm, cudaStream_t st);
+
+}  // namespace vlx

@@ -26,15 +26,15 @@
 #include <vector>
 
 #include "vlx_b200.h"
-#include "vlx_interp.cuh"
+#include "vlx_coop.cuh"
 #include "vlx_kernels.cuh"
 #include "dispatch.inc"
 
-extern "C" const char vlx_interp_blob_start[];
-extern "C" const char vlx_interp_blob_end[];
+extern "C" const char vlx_coop_blob_start[];
+extern "C" const char vlx_coop_blob_end[];
 
 using vlx::FockArgs;
-using vlx::InterpClassDev;
+using vlx::CoopClassDev;
 using vlx::PairBlockDev;
 using vlx::WorkItem;
 
@@ -125,7 +125,8 @@ struct DeviceGlobals {
     int nsm = 0;
     double* boys = nullptr;
     void* prog = nullptr;
-    std::vector<InterpClassDev> interp;
+    std::vector<CoopClassDev> coop;
+    std::vector<int> coop_prim_flops, coop_post_flops;
 };
 
 std::mutex g_dev_mutex;
@@ -141,55 +142,70 @@ int device_globals(int device, DeviceGlobals** out)
         const auto tab = make_boys_table();
         VLX_CUDA(cudaMalloc(&g.boys, tab.size() * sizeof(double)));
         VLX_CUDA(cudaMemcpy(g.boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
-        // interpreter programs: int32 header, per class 14 int32, ops (8 int32 + 2 double), outs
-        const char* blob = vlx_interp_blob_start;
-        const size_t bsize = (size_t)(vlx_interp_blob_end - vlx_interp_blob_start);
+        // warp-cooperative programs (gen_coop.py): magic, count, 14-int headers,
+        // 64-byte op records (8 int32 + 4 float64), then the aux int32 stream
+        const char* blob = vlx_coop_blob_start;
+        const size_t bsize = (size_t)(vlx_coop_blob_end - vlx_coop_blob_start);
         int head[2];
         std::memcpy(head, blob, sizeof(head));
-        if (head[0] != 0x564C5850) return fail(VLX_B200_ERR_CUDA, "corrupt interpreter program blob");
+        if (head[0] != 0x434F4F50) return fail(VLX_B200_ERR_CUDA, "corrupt cooperative program blob");
         const int ncls = head[1];
-        std::vector<int> ch((size_t)ncls * 14);
+        constexpr int HW = 14;
+        std::vector<int> ch((size_t)ncls * HW);
         std::memcpy(ch.data(), blob + 8, ch.size() * sizeof(int));
-        size_t nops = 0, nout = 0;
+        size_t nops = 0, naux = 0;
         for (int c = 0; c < ncls; c++) {
-            nops += ch[c * 14 + 4] + ch[c * 14 + 5] + ch[c * 14 + 6];
-            nout += ch[c * 14 + 10];
+            const int* h = &ch[c * HW];
+            nops += h[6] + h[7];
+            const int L = h[0] + h[1] + h[2] + h[3];
+            const int nsph = (2 * h[0] + 1) * (2 * h[1] + 1) * (2 * h[2] + 1) * (2 * h[3] + 1);
+            naux += (h[8] + 2) + (h[9] + 2) + (L + 1) + nsph;
         }
         const char* ops = blob + 8 + ch.size() * sizeof(int);
-        const char* outs = ops + nops * 48;
-        if ((size_t)(outs + nout * 4 - blob) > bsize) return fail(VLX_B200_ERR_CUDA, "truncated program blob");
+        const char* aux = ops + nops * 64;
+        if ((size_t)(aux + naux * 4 - blob) > bsize) return fail(VLX_B200_ERR_CUDA, "truncated program blob");
         std::vector<int> opi(nops * 8);
-        std::vector<double> opd(nops * 2);
+        std::vector<double> opw(nops * 4);
         for (size_t o = 0; o < nops; o++) {
-            std::memcpy(&opi[o * 8], ops + o * 48, 32);
-            std::memcpy(&opd[o * 2], ops + o * 48 + 32, 16);
+            std::memcpy(&opi[o * 8], ops + o * 64, 32);
+            std::memcpy(&opw[o * 4], ops + o * 64 + 32, 32);
         }
-        const size_t bytes_i = opi.size() * 4, bytes_d = opd.size() * 8, bytes_o = nout * 4;
+        const size_t bytes_i = opi.size() * 4, bytes_w = opw.size() * 8, bytes_a = naux * 4;
         char* dev = nullptr;
-        VLX_CUDA(cudaMalloc(&dev, bytes_i + bytes_d + bytes_o + 64));
+        VLX_CUDA(cudaMalloc(&dev, bytes_i + bytes_w + bytes_a + 64));
         VLX_CUDA(cudaMemcpy(dev, opi.data(), bytes_i, cudaMemcpyHostToDevice));
-        VLX_CUDA(cudaMemcpy(dev + bytes_i, opd.data(), bytes_d, cudaMemcpyHostToDevice));
-        VLX_CUDA(cudaMemcpy(dev + bytes_i + bytes_d, outs, bytes_o, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMemcpy(dev + bytes_i, opw.data(), bytes_w, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMemcpy(dev + bytes_i + bytes_w, aux, bytes_a, cudaMemcpyHostToDevice));
         g.prog = dev;
+        const int* daux = reinterpret_cast<const int*>(dev + bytes_i + bytes_w);
         for (int c = 0; c < ncls; c++) {
-            const int* h = &ch[c * 14];
-            InterpClassDev d;
+            const int* h = &ch[c * HW];
+            CoopClassDev d;
             d.la = h[0];
             d.lb = h[1];
             d.lc = h[2];
             d.ld = h[3];
-            d.nvrr = h[4];
-            d.nacc_ops = h[5];
-            d.npost = h[6];
-            d.nslots = h[7];
-            d.acc_first = h[8];
-            d.nacc = h[9];
-            d.nout = h[10];
-            d.opi = reinterpret_cast<const int4*>(dev) + (size_t)h[11] * 2;
-            d.opd = reinterpret_cast<const double2*>(dev + bytes_i) + h[11];
-            d.out = reinterpret_cast<const int*>(dev + bytes_i + bytes_d) + h[12];
-            g.interp.push_back(d);
+            d.nslots = h[4];
+            d.nacc = h[5];
+            d.nbody = h[6];
+            d.npost = h[7];
+            d.nblev = h[8];
+            d.nplev = h[9];
+            d.opi = reinterpret_cast<const int4*>(dev) + (size_t)h[10] * 2;
+            d.opw = reinterpret_cast<const double2*>(dev + bytes_i) + (size_t)h[10] * 2;
+            // level offsets index the class's op array (post offsets already
+            // rebased after the body ops by the generator)
+            const int* a0 = daux + h[11];
+            d.boff = a0;
+            d.poff = a0 + (h[8] + 2);
+            const int L = h[0] + h[1] + h[2] + h[3];
+            d.fslots = d.poff + (h[9] + 2);
+            d.outs = d.fslots + (L + 1);
+            g.coop.push_back(d);
+            g.coop_prim_flops.push_back(h[12]);
+            g.coop_post_flops.push_back(h[13]);
         }
+        VLX_CUDA(vlx::coop_prepare());
         g.ready = true;
     }
     *out = &g;
@@ -231,6 +247,18 @@ void launch_boys_test(int m, const double* T, double* F, int n, const double* ta
         launch_boys_test<M - 1>(m, T, F, n, tab);
 }
 
+// FP64 throughput probe: 8 independent FMA chains per thread.
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b)
+{
+    double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; i++) {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    const double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (r == 12345.678) out[threadIdx.x] = r;
+}
+
 // ------------------------------------------------------------------ screener state
 struct Shell {
     double xyz[3];
@@ -249,9 +277,11 @@ struct PairBlock {
 
 struct ClassTasks {
     int compiled = -1;  // index into kQuartetClasses
-    int interp = -1;    // index into DeviceGlobals::interp
+    int coop = -1;      // index into DeviceGlobals::coop
+    int la = 0, lb = 0, lc = 0, ld = 0;
     std::vector<WorkItem> items;
     size_t offset = 0;
+    long long quartets = 0, prim_quartets = 0;
 };
 
 struct TaskSet {
@@ -262,6 +292,9 @@ struct TaskSet {
 };
 
 int pair_key(int la, int lb) { return (la + lb) * 16 + lb; }
+
+// ket pairs per work item of a warp-cooperative class
+constexpr int kCoopSegment = 2;
 
 }  // namespace
 
@@ -281,8 +314,6 @@ struct vlx_b200_screener {
     double* d_acc = nullptr;
     int* d_counters = nullptr;
     int ncounters = 0;
-    double* d_scratch = nullptr;
-    size_t scratch_bytes = 0;
     int seg = 256;
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -378,34 +409,13 @@ int find_compiled(int la, int lb, int lc, int ld)
     return -1;
 }
 
-int find_interp(const DeviceGlobals* g, int la, int lb, int lc, int ld)
+int find_coop(const DeviceGlobals* g, int la, int lb, int lc, int ld)
 {
-    for (size_t c = 0; c < g->interp.size(); c++) {
-        const auto& e = g->interp[c];
+    for (size_t c = 0; c < g->coop.size(); c++) {
+        const auto& e = g->coop[c];
         if (e.la == la && e.lb == lb && e.lc == lc && e.ld == ld) return (int)c;
     }
     return -1;
-}
-
-// Scratch of the table-driven kernel: nslots doubles per resident thread,
-// capped at 2 GiB (the grid shrinks instead).
-int interp_grid(vlx_b200_screener* s, const InterpClassDev& c, int threads_per_block, int want_blocks, int* grid)
-{
-    const size_t per_thread = (size_t)c.nslots * sizeof(double);
-    const size_t cap = size_t(2) << 30;
-    int blocks = std::min(want_blocks, s->glob->nsm * 4);
-    while (blocks > 1 && per_thread * blocks * threads_per_block > cap) blocks--;
-    blocks = std::max(blocks, 1);
-    const size_t need = per_thread * blocks * threads_per_block;
-    if (need > s->scratch_bytes) {
-        if (s->d_scratch) cudaFree(s->d_scratch);
-        s->d_scratch = nullptr;
-        s->scratch_bytes = 0;
-        VLX_CUDA(cudaMalloc(&s->d_scratch, need));
-        s->scratch_bytes = need;
-    }
-    *grid = blocks;
-    return VLX_B200_OK;
 }
 
 int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
@@ -423,15 +433,11 @@ int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
                 done = true;
             }
         }
-        if (!done) {
-            const int ic = find_interp(s->glob, pb.la, pb.lb, pb.la, pb.lb);
+        if (!done && n > 0) {
+            const int ic = find_coop(s->glob, pb.la, pb.lb, pb.la, pb.lb);
             if (ic < 0) return fail(VLX_B200_ERR_UNSUPPORTED, "no kernel for Schwarz class");
-            int grid = 0;
-            const int want = (n + 63) / 64;
-            int rc = interp_grid(s, s->glob->interp[ic], 64, std::max(1, want), &grid);
-            if (rc) return rc;
-            vlx::launch_interp_schwarz(s->d_blocks, (int)b, s->glob->interp[ic], s->glob->boys, s->d_scratch, grid,
-                                       d_max[b], s->stream);
+            vlx::launch_coop_schwarz(s->d_blocks, (int)b, n, s->glob->coop[ic], s->glob->boys, d_max[b],
+                                     s->glob->nsm, s->stream);
         }
         VLX_CUDA(cudaGetLastError());
     }
@@ -474,9 +480,13 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
             auto it = cls_index.find(key);
             if (it == cls_index.end()) {
                 ClassTasks ct;
+                ct.la = Pb.la;
+                ct.lb = Pb.lb;
+                ct.lc = Pk.la;
+                ct.ld = Pk.lb;
                 ct.compiled = find_compiled(Pb.la, Pb.lb, Pk.la, Pk.lb);
-                if (ct.compiled < 0) ct.interp = find_interp(s->glob, Pb.la, Pb.lb, Pk.la, Pk.lb);
-                if (ct.compiled < 0 && ct.interp < 0)
+                if (ct.compiled < 0) ct.coop = find_coop(s->glob, Pb.la, Pb.lb, Pk.la, Pk.lb);
+                if (ct.compiled < 0 && ct.coop < 0)
                     return fail(VLX_B200_ERR_UNSUPPORTED, "quartet class not compiled in");
                 it = cls_index.emplace(key, (int)ts.classes.size()).first;
                 ts.classes.push_back(ct);
@@ -491,8 +501,11 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                 if (kmax < 0) break;
                 const int kend = Pk.bin_off[std::min(kmax, 15) + 1];
                 const int kbeg = diag ? x : 0;
-                for (int k0 = kbeg; k0 < kend; k0 += s->seg) {
-                    const int k1 = std::min(kend, k0 + s->seg);
+                // a compiled-class item feeds 32 lanes per step; a cooperative-class
+                // item is walked one quartet at a time by one warp, so it stays short
+                const int seg = (ct.coop >= 0) ? kCoopSegment : s->seg;
+                for (int k0 = kbeg; k0 < kend; k0 += seg) {
+                    const int k1 = std::min(kend, k0 + seg);
                     if ((g++ % nodes) != rank) continue;
                     WorkItem w;
                     w.blocks = (int)bra | ((int)ket << 16);
@@ -502,6 +515,8 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                     ct.items.push_back(w);
                     ts.quartets += k1 - k0;
                     ts.prim_quartets += (long long)(k1 - k0) * kp;
+                    ct.quartets += k1 - k0;
+                    ct.prim_quartets += (long long)(k1 - k0) * kp;
                 }
             }
         }
@@ -557,7 +572,8 @@ int ensure_buffers(vlx_b200_screener* s)
 
 // Enqueues all class kernels of a task set on `st`; F (accumulator) must be zeroed.
 int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
-                    double cj, double ck, cudaStream_t st, long long* launches)
+                    double cj, double ck, cudaStream_t st, long long* launches,
+                    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
 {
     if (ts->classes.empty()) return VLX_B200_OK;
     VLX_CUDA(cudaMemsetAsync(s->d_counters, 0, ts->classes.size() * sizeof(int), st));
@@ -580,21 +596,42 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
         a.nitems = (int)ct.items.size();
         a.counter = s->d_counters + c;
         const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
+        if (events) VLX_CUDA(cudaEventRecord((*events)[c].first, st));
         if (ct.compiled >= 0) {
             const auto& e = vlx::kQuartetClasses[ct.compiled];
             const int occ = std::max(1, e.occupancy(mode));
             const int grid = std::max(1, std::min(want, occ * s->glob->nsm));
             e.launch(mode, a, grid, st);
         } else {
-            int grid = 0;
-            int rc = interp_grid(s, s->glob->interp[ct.interp], 128, std::max(1, want), &grid);
-            if (rc) return rc;
-            vlx::launch_interp_quartet(mode, a, s->glob->interp[ct.interp], s->d_scratch, grid, st);
+            const CoopClassDev& cc = s->glob->coop[ct.coop];
+            const int wpb = vlx::coop_warps_per_block(cc);
+            const int cap = vlx::coop_blocks_per_sm(cc) * s->glob->nsm;
+            const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
+            vlx::launch_coop_quartet(mode, a, cc, grid, st);
         }
         VLX_CUDA(cudaGetLastError());
+        if (events) VLX_CUDA(cudaEventRecord((*events)[c].second, st));
         if (launches) (*launches)++;
     }
     return VLX_B200_OK;
+}
+
+// Algorithmic FP64 flops of one class launch: per primitive quartet the
+// recursion graph + Boys (28 + 3M) + geometric factors (30); per contracted
+// quartet HRR + spherical transforms + digestion (12 per spherical integral).
+double class_flops(const vlx_b200_screener* s, const ClassTasks& ct)
+{
+    int pf = 0, qf = 0;
+    if (ct.compiled >= 0) {
+        pf = vlx::kQuartetClasses[ct.compiled].prim_flops;
+        qf = vlx::kQuartetClasses[ct.compiled].post_flops;
+    } else {
+        pf = s->glob->coop_prim_flops[ct.coop];
+        qf = s->glob->coop_post_flops[ct.coop];
+    }
+    const int M = ct.la + ct.lb + ct.lc + ct.ld;
+    const double nsph = (2.0 * ct.la + 1) * (2 * ct.lb + 1) * (2 * ct.lc + 1) * (2 * ct.ld + 1);
+    return (double)ct.prim_quartets * (pf + 28 + 3 * M + 30) + (double)ct.quartets * (qf + 12.0 * nsph);
 }
 
 int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, int symmetric, const char* label,
@@ -819,7 +856,6 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_F) cudaFree(s->d_F);
     if (s->d_acc) cudaFree(s->d_acc);
     if (s->d_counters) cudaFree(s->d_counters);
-    if (s->d_scratch) cudaFree(s->d_scratch);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -934,6 +970,98 @@ int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
     }
     cudaFree(d_eri);
     return rc;
+}
+
+int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int symmetric, const char* label,
+                          double xfac, int ith, double* d_fock, void* stream, int max_classes,
+                          vlx_b200_class_profile* out, int* nclasses)
+{
+    if (!s || !d_density || !d_fock || !out || !nclasses || max_classes < 1)
+        return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    VLX_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    double cj = 0.0, ck = 0.0;
+    if (!label_weights(label, symmetric, xfac, &cj, &ck)) return fail(VLX_B200_ERR_ARGUMENT, "unknown label");
+    int rc = ensure_buffers(s);
+    if (rc) return rc;
+    TaskSet* ts = nullptr;
+    rc = build_tasks(s, ith, 0, 1, &ts);
+    if (rc) return rc;
+    const size_t nc = ts->classes.size();
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev(nc);
+    for (auto& e : ev) {
+        VLX_CUDA(cudaEventCreate(&e.first));
+        VLX_CUDA(cudaEventCreate(&e.second));
+    }
+    const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
+    rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
+                         cj, ck, st, nullptr, &ev);
+    if (!rc && symmetric) {
+        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
+    } else if (!rc) {
+        cudaMemcpyAsync(d_fock, s->d_acc, bytes, cudaMemcpyDeviceToDevice, st);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    int n = 0;
+    for (size_t c = 0; c < nc && !rc; c++) {
+        const ClassTasks& ct = ts->classes[c];
+        if (ct.items.empty()) continue;
+        if (n >= max_classes) break;
+        vlx_b200_class_profile& p = out[n++];
+        p.la = ct.la;
+        p.lb = ct.lb;
+        p.lc = ct.lc;
+        p.ld = ct.ld;
+        p.table_driven = ct.compiled < 0 ? 1 : 0;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
+        p.device_ms = ms;
+        p.shell_quartets = ct.quartets;
+        p.prim_quartets = ct.prim_quartets;
+        p.flops = class_flops(s, ct);
+    }
+    for (auto& x : ev) {
+        cudaEventDestroy(x.first);
+        cudaEventDestroy(x.second);
+    }
+    *nclasses = n;
+    return rc;
+}
+
+int vlx_b200_fp64_peak(int device, double* tflops)
+{
+    if (!tflops) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    DeviceGlobals* g = nullptr;
+    int rc = device_globals(device, &g);
+    if (rc) return rc;
+    VLX_CUDA(cudaSetDevice(device));
+    double* d = nullptr;
+    VLX_CUDA(cudaMalloc(&d, 1024 * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int iters = 4096, blocks = g->nsm * 8, threads = 256;
+    fp64_probe_kernel<<<blocks, threads>>>(d, 64, 1.0000001, 1e-9);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+        cudaEventRecord(e0);
+        fp64_probe_kernel<<<blocks, threads>>>(d, iters, 1.0000001, 1e-9);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3) / 1e12;
+    return VLX_B200_OK;
 }
 
 int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F)
