@@ -120,6 +120,38 @@ int vlx_b200_fock_build_device(vlx_b200_screener* screener, const double* d_dens
                                const char* label, double exchange_factor, double omega, int ithreshold,
                                double* d_fock, void* stream);
 
+/* Largest basis accepted by vlx_b200_fock_build_noalloc. */
+#define VLX_B200_NOALLOC_MAX_NAO 1024
+
+/* Device-resident build that allocates no device memory.  It has no
+ * counterpart in the reference.
+ *
+ * Some callers cannot let a library call cudaMalloc during a build: a host
+ * application whose own pool allocator already owns the GPU memory (a
+ * framework holding most of HBM, or fixed per-rank pools in an MPI job), or a
+ * caller that runs other streams next to the Fock build and cannot afford the
+ * device-wide synchronisation that cudaFree implies.  This entry point takes
+ * its scratch (the FP64 Fock accumulator and the work-queue heads) from a
+ * static device array of the library instead: 8 MiB, held by every GPU that
+ * loads the library until the process exits, enough for nao <= 1024.
+ *
+ * d_density / d_fock: device pointers (nao x nao) on the screener's device;
+ * stream: cudaStream_t (NULL = the screener's own stream); label, ithreshold,
+ * exchange_factor, omega as in vlx_b200_fock_build.  Returns when the work is
+ * enqueued.  Limits and behaviour:
+ *  - nao above VLX_B200_NOALLOC_MAX_NAO is rejected with VLX_B200_ERR_ARGUMENT;
+ *  - the screener must already hold the work list of `ithreshold`: one
+ *    ordinary build (vlx_b200_fock_build*) with that threshold creates it;
+ *    otherwise VLX_B200_ERR_ARGUMENT;
+ *  - the first call on a device looks up the address of the static array on
+ *    that device, so make that first call before any stream capture;
+ *  - all calls share the one array, which keeps the previous call's contents
+ *    (each call clears what it needs): calls that overlap on the GPU, from
+ *    two streams or two screeners, race and give wrong results. */
+int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_density, int symmetric,
+                                const char* label, double exchange_factor, double omega, int ithreshold,
+                                double* d_fock, void* stream);
+
 /* Dense (nao)^4 ERI tensor over the screened unique quartets (all eight
  * index permutations written), host buffer.
  * Replaces CFockDriver::compute_eri(screener, nao, ithreshold)

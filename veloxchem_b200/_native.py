@@ -44,6 +44,8 @@ SIGNATURES = {
     'vlx_b200_fock_profile': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double, ctypes.c_int,
                                              _vp, _vp, ctypes.c_int, _vp, _ip]),
     'vlx_b200_fp64_peak': (ctypes.c_int, [ctypes.c_int, _dp]),
+    'vlx_b200_fock_build_noalloc': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_int, _vp, _vp]),
 }
 
 

@@ -948,6 +948,121 @@ int vlx_b200_fock_build_device(vlx_b200_screener* s, const double* d_density, in
     return device_build(s, 0, 1, d_density, symmetric, label, xfac, omega, ith, d_fock, st, nullptr, nullptr, nullptr);
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free build
+// Scratch of vlx_b200_fock_build_noalloc: the FP64 Fock accumulator (at most
+// VLX_B200_NOALLOC_MAX_NAO^2 values, 8 MiB) and the work-queue heads of the
+// class launches live in static device arrays instead of cudaMalloc'd buffers.
+// Every device that loads the library holds these 8 MiB until the process
+// exits; all calls share them.
+namespace {
+
+constexpr int kNoallocMaxClasses = 64;
+static __device__ __align__(256) double g_noalloc_acc[(size_t)VLX_B200_NOALLOC_MAX_NAO * VLX_B200_NOALLOC_MAX_NAO];
+static __device__ __align__(256) int g_noalloc_heads[kNoallocMaxClasses];
+
+struct NoallocScratch {
+    double* acc = nullptr;
+    int* heads = nullptr;
+};
+std::mutex g_noalloc_mutex;
+std::map<int, NoallocScratch> g_noalloc;  // per device: device addresses of the static arrays
+
+// Device addresses of the static arrays on `device` (looked up once, with the
+// device current; host code must not use the symbols themselves as pointers).
+int noalloc_scratch(int device, NoallocScratch* out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    auto it = g_noalloc.find(device);
+    if (it == g_noalloc.end()) {
+        NoallocScratch sc;
+        VLX_CUDA(cudaSetDevice(device));
+        VLX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.acc), g_noalloc_acc));
+        VLX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.heads), g_noalloc_heads));
+        it = g_noalloc.emplace(device, sc).first;
+    }
+    *out = it->second;
+    return VLX_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, int symmetric, const char* label,
+                                double xfac, double omega, int ith, double* d_fock, void* stream)
+{
+    if (!s || !d_density || !d_fock) return fail(VLX_B200_ERR_ARGUMENT, "fock_build_noalloc: null argument");
+    if (s->nao > VLX_B200_NOALLOC_MAX_NAO)
+        return fail(VLX_B200_ERR_ARGUMENT, "fock_build_noalloc: " + std::to_string(s->nao) +
+                                               " basis functions exceed the static scratch limit of " +
+                                               std::to_string(VLX_B200_NOALLOC_MAX_NAO));
+    if (omega != 0.0) return fail(VLX_B200_ERR_UNSUPPORTED, "range-separated (omega != 0) integrals not compiled in");
+    double cj = 0.0, ck = 0.0;
+    const bool known = label_weights(label, symmetric, xfac, &cj, &ck);
+    // the work list must already exist: building it would allocate device memory
+    TaskSet* ts = nullptr;
+    for (auto& t : s->tasksets)
+        if (t.ith == ith && t.rank == 0 && t.nodes == 1 && t.seg == s->seg) ts = &t;
+    if (known && !ts)
+        return fail(VLX_B200_ERR_ARGUMENT,
+                    "fock_build_noalloc: no work list for ithreshold " + std::to_string(ith) +
+                        " on this screener; run one allocating build (vlx_b200_fock_build*) with it first");
+    if (ts && ts->classes.size() > (size_t)kNoallocMaxClasses)
+        return fail(VLX_B200_ERR_UNSUPPORTED, "fock_build_noalloc: too many quartet classes");
+    VLX_CUDA(cudaSetDevice(s->device));
+    NoallocScratch sc;
+    int rc = noalloc_scratch(s->device, &sc);
+    if (rc) return rc;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    // the arrays keep the previous call's contents: clear the accumulator and the queue heads
+    VLX_CUDA(cudaMemsetAsync(sc.acc, 0, bytes, st));
+    if (known && !ts->classes.empty()) {
+        VLX_CUDA(cudaMemsetAsync(sc.heads, 0, ts->classes.size() * sizeof(int), st));
+        FockArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.blocks = s->d_blocks;
+        a.boys = s->glob->boys;
+        a.D = d_density;
+        a.F = sc.acc;
+        a.nao = s->nao;
+        for (int l = 0; l <= VLX_LMAX; l++) a.nl[l] = s->nl[l];
+        a.cj = cj;
+        a.ck = ck;
+        const int mode = symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN;
+        for (size_t c = 0; c < ts->classes.size(); c++) {
+            const ClassTasks& ct = ts->classes[c];
+            if (ct.items.empty()) continue;
+            a.items = ts->d_items + ct.offset;
+            a.nitems = (int)ct.items.size();
+            a.counter = sc.heads + c;
+            if (ct.compiled >= 0) {
+                const auto& e = vlx::kQuartetClasses[ct.compiled];
+                const int want = (int)((ct.items.size() + vlx::kWarpsPerBlock - 1) / vlx::kWarpsPerBlock);
+                const int grid = std::max(1, std::min(want, std::max(1, e.occupancy(mode)) * s->glob->nsm));
+                e.launch(mode, a, grid, st);
+            } else {
+                const CoopClassDev& cc = s->glob->coop[ct.coop];
+                const int wpb = vlx::coop_warps_per_block(cc);
+                const int cap = vlx::coop_blocks_per_sm(cc) * s->glob->nsm;
+                const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
+                vlx::launch_coop_quartet(mode, a, cc, grid, st);
+            }
+            VLX_CUDA(cudaGetLastError());
+        }
+    }
+    if (symmetric) {
+        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(sc.acc, d_fock, s->nao);
+        VLX_CUDA(cudaGetLastError());
+    } else {
+        VLX_CUDA(cudaMemcpyAsync(d_fock, sc.acc, bytes, cudaMemcpyDeviceToDevice, st));
+    }
+    return VLX_B200_OK;
+}
+
 int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
 {
     if (!s || !eri_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
