@@ -120,6 +120,18 @@ class ClockSampler:
                 'samples': len(sm)}
 
 
+def _profiled_traffic(cls):
+    """DRAM bytes per launch of a class kernel from its committed ncu summary
+    (profiles/quartet_kernel_<class>_h2o32_svp.md), or None."""
+    import re
+    name = '%d%d%d%d' % (cls['la'], cls['lb'], cls['lc'], cls['ld'])
+    path = ROOT / 'profiles' / ('quartet_kernel_%s_h2o32_svp.md' % name)
+    if not path.exists():
+        return None
+    m = re.search(r'dram_bytes_per_launch:\s*(\d+)', path.read_text())
+    return int(m.group(1)) if m else None
+
+
 def cpu_reference_build(mol, bas, dens, nodes=1, threads=None):
     """Seconds for the reference FockDriver share (rank 0 of `nodes`) on host cores."""
     from oracle.oracle import RefOracle
@@ -234,7 +246,7 @@ def run_ours(args):
     achieved = top['flops'] / (top['device_ms'] * 1e-3) / 1e12
     all_flops = sum(p['flops'] for p in prof)
     roofline = {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
-                'traffic': None,
+                'traffic': _profiled_traffic(top),
                 'kernel': 'quartet_kernel<%d,%d,%d,%d>' % (top['la'], top['lb'], top['lc'], top['ld']),
                 'kernel_share': top['device_ms'] / tot_prof_ms,
                 'peak_source': 'measured: FP64 FMA-chain probe kernel (vlx_b200_fp64_peak), burst; '

@@ -292,44 +292,54 @@ class CoopProgram:
         return body, offsets(body, self.body_levels), post, offsets(post, self.post_levels)
 
     def pack(self):
+        """16-byte op records: int32 {dst | x << 16, y | u << 16, v | w << 16,
+        kind*4+axis | c1 << 8 | c2 << 16}; a LIN op keeps its 3 weights in the
+        class's weight array and their index in the (v | w << 16) word."""
         s = self.slot
         body, boff, post, poff = self.records()
-        ints, dbls = [], []
+        ints, lw = [], []
         for o in body + post:
             src = [s[x] for x in o.src] + [0] * (5 - len(o.src))
-            ints.append(struct.pack('<8i', o.kind * 4 + o.axis, s[o.dst], src[0], src[1], src[2], src[3], src[4],
-                                    (o.c1 & 0xff) | ((o.c2 & 0xff) << 8)))
-            dbls.append(struct.pack('<4d', o.w[0], o.w[1], o.w[2], 0.0))
+            assert max(src + [s[o.dst]]) < 65536
+            if o.kind == 5:
+                word2 = len(lw) // 3
+                lw.extend(o.w)
+            else:
+                word2 = src[3] | (src[4] << 16)
+            ints.append(struct.pack('<4i', s[o.dst] | (src[0] << 16), src[1] | (src[2] << 16), word2,
+                                    (o.kind * 4 + o.axis) | ((o.c1 & 0xff) << 8) | ((o.c2 & 0xff) << 16)))
         fslots = [s[self.fvals[m]] if m in self.fvals else 0 for m in range(self.L + 1)]
         outs = [s[v] for v in self.out]
-        return dict(ints=b''.join(ints), dbls=b''.join(dbls), nbody=len(body), npost=len(post),
+        return dict(ints=b''.join(ints), lw=lw, nbody=len(body), npost=len(post),
                     boff=boff, poff=poff, fslots=fslots, outs=outs, nslots=self.nslots, nacc=len(self.acc))
 
 
 def emit_blob(classes, path):
     """Binary blob of the cooperative programs (embedded by vlx_blob.S).
 
-    int32 magic 0x434F4F50, int32 count; per class 14 int32 header
+    int32 magic 0x434F4F51, int32 count; per class 16 int32 header
     (la lb lc ld nslots nacc nbody npost nbody_levels npost_levels op_offset
-    aux_offset prim_flops post_flops); then all op records (8 int32 + 4 float64 = 64 bytes each);
-    then the aux int32 stream per class: body level offsets (nbody_levels + 2),
-    post level offsets (npost_levels + 2), F slots (L + 1), output slots."""
-    heads, ops, aux = [], [], []
-    nops = naux = 0
+    aux_offset prim_flops post_flops weight_offset nweights); then all op
+    records (4 int32 each); then all LIN weights (float64); then the aux int32
+    stream per class: body level offsets (nbody_levels + 2), post level offsets
+    rebased after the body ops (npost_levels + 2), F slots (L + 1), output slots."""
+    heads, ops, wts, aux = [], [], [], []
+    nops = naux = nw = 0
     for cls in classes:
         p = CoopProgram(*cls)
         r = p.pack()
-        # post offsets are rebased after the body ops (one op array per class)
         a = r['boff'] + [x + r['nbody'] for x in r['poff']] + r['fslots'] + r['outs']
         fv, fa, fp = p.g.flops()
-        heads.append(struct.pack('<14i', *cls, r['nslots'], r['nacc'], r['nbody'], r['npost'], len(r['boff']) - 2,
-                                 len(r['poff']) - 2, nops, naux, fv + fa, fp))
-        for k in range(r['nbody'] + r['npost']):
-            ops.append(r['ints'][32 * k:32 * k + 32] + r['dbls'][32 * k:32 * k + 32])
+        heads.append(struct.pack('<16i', *cls, r['nslots'], r['nacc'], r['nbody'], r['npost'], len(r['boff']) - 2,
+                                 len(r['poff']) - 2, nops, naux, fv + fa, fp, nw, len(r['lw'])))
+        ops.append(r['ints'])
+        wts.append(struct.pack('<%dd' % len(r['lw']), *r['lw']))
         aux.append(struct.pack('<%di' % len(a), *a))
         nops += r['nbody'] + r['npost']
         naux += len(a)
-    blob = struct.pack('<2i', 0x434F4F50, len(classes)) + b''.join(heads) + b''.join(ops) + b''.join(aux)
+        nw += len(r['lw'])
+    blob = (struct.pack('<2i', 0x434F4F51, len(classes)) + b''.join(heads) + b''.join(ops) + b''.join(wts) +
+            b''.join(aux))
     if not path.exists() or path.read_bytes() != blob:
         path.write_bytes(blob)
 

@@ -9,8 +9,9 @@ namespace vlx {
 struct CoopClassDev {
     int la, lb, lc, ld;
     int nslots, nacc, nbody, npost, nblev, nplev;
-    const int4* opi;     // 2 x int4 per op: {kind*4+axis, dst, x, y}, {u, v, w, c1 | c2 << 8}
-    const double2* opw;  // 2 x double2 per op: {w0, w1}, {w2, 0}
+    const int4* ops;     // per op {dst | x << 16, y | u << 16, v | w << 16 (LIN: weight index),
+                         //         kind*4+axis | c1 << 8 | c2 << 16}
+    const double* lw;    // LIN weights, 3 per LIN op
     const int* boff;     // body level offsets (index l = first op of level l; levels 1..nblev)
     const int* poff;     // post level offsets
     const int* fslots;   // slot of pref * F_m, m = 0..la+lb+lc+ld (0 = unused)

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -106,7 +107,8 @@ std::vector<double> make_boys_table()
             long double fv[BOYS_NCOEF];
             for (int k = 0; k < N; k++) {
                 const long double x = std::cos(M_PI * (k + 0.5L) / N);
-                fv[k] = boys_series(m, it + 0.5L + 0.5L * x);
+                const long double h = 1.0L / BOYS_INV_H;
+                fv[k] = boys_series(m, it * h + 0.5L * h + 0.5L * h * x);
             }
             for (int j = 0; j < N; j++) {
                 long double s = 0.0L;
@@ -142,42 +144,39 @@ int device_globals(int device, DeviceGlobals** out)
         const auto tab = make_boys_table();
         VLX_CUDA(cudaMalloc(&g.boys, tab.size() * sizeof(double)));
         VLX_CUDA(cudaMemcpy(g.boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
-        // warp-cooperative programs (gen_coop.py): magic, count, 14-int headers,
-        // 64-byte op records (8 int32 + 4 float64), then the aux int32 stream
+        // warp-cooperative programs (gen_coop.py): magic, count, 16-int headers,
+        // 16-byte op records, LIN weights (float64), then the aux int32 stream
         const char* blob = vlx_coop_blob_start;
         const size_t bsize = (size_t)(vlx_coop_blob_end - vlx_coop_blob_start);
         int head[2];
         std::memcpy(head, blob, sizeof(head));
-        if (head[0] != 0x434F4F50) return fail(VLX_B200_ERR_CUDA, "corrupt cooperative program blob");
+        if (head[0] != 0x434F4F51) return fail(VLX_B200_ERR_CUDA, "corrupt cooperative program blob");
         const int ncls = head[1];
-        constexpr int HW = 14;
+        constexpr int HW = 16;
         std::vector<int> ch((size_t)ncls * HW);
         std::memcpy(ch.data(), blob + 8, ch.size() * sizeof(int));
-        size_t nops = 0, naux = 0;
+        size_t nops = 0, naux = 0, nwts = 0;
         for (int c = 0; c < ncls; c++) {
             const int* h = &ch[c * HW];
             nops += h[6] + h[7];
+            nwts += h[15];
             const int L = h[0] + h[1] + h[2] + h[3];
             const int nsph = (2 * h[0] + 1) * (2 * h[1] + 1) * (2 * h[2] + 1) * (2 * h[3] + 1);
             naux += (h[8] + 2) + (h[9] + 2) + (L + 1) + nsph;
         }
         const char* ops = blob + 8 + ch.size() * sizeof(int);
-        const char* aux = ops + nops * 64;
+        const char* wts = ops + nops * 16;
+        const char* aux = wts + nwts * 8;
         if ((size_t)(aux + naux * 4 - blob) > bsize) return fail(VLX_B200_ERR_CUDA, "truncated program blob");
-        std::vector<int> opi(nops * 8);
-        std::vector<double> opw(nops * 4);
-        for (size_t o = 0; o < nops; o++) {
-            std::memcpy(&opi[o * 8], ops + o * 64, 32);
-            std::memcpy(&opw[o * 4], ops + o * 64 + 32, 32);
-        }
-        const size_t bytes_i = opi.size() * 4, bytes_w = opw.size() * 8, bytes_a = naux * 4;
+        const size_t bytes_o = nops * 16, bytes_w = nwts * 8, bytes_a = naux * 4;
+        const size_t off_w = (bytes_o + 255) & ~size_t(255), off_a = off_w + ((bytes_w + 255) & ~size_t(255));
         char* dev = nullptr;
-        VLX_CUDA(cudaMalloc(&dev, bytes_i + bytes_w + bytes_a + 64));
-        VLX_CUDA(cudaMemcpy(dev, opi.data(), bytes_i, cudaMemcpyHostToDevice));
-        VLX_CUDA(cudaMemcpy(dev + bytes_i, opw.data(), bytes_w, cudaMemcpyHostToDevice));
-        VLX_CUDA(cudaMemcpy(dev + bytes_i + bytes_w, aux, bytes_a, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMalloc(&dev, off_a + bytes_a + 64));
+        VLX_CUDA(cudaMemcpy(dev, ops, bytes_o, cudaMemcpyHostToDevice));
+        if (bytes_w) VLX_CUDA(cudaMemcpy(dev + off_w, wts, bytes_w, cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMemcpy(dev + off_a, aux, bytes_a, cudaMemcpyHostToDevice));
         g.prog = dev;
-        const int* daux = reinterpret_cast<const int*>(dev + bytes_i + bytes_w);
+        const int* daux = reinterpret_cast<const int*>(dev + off_a);
         for (int c = 0; c < ncls; c++) {
             const int* h = &ch[c * HW];
             CoopClassDev d;
@@ -191,8 +190,8 @@ int device_globals(int device, DeviceGlobals** out)
             d.npost = h[7];
             d.nblev = h[8];
             d.nplev = h[9];
-            d.opi = reinterpret_cast<const int4*>(dev) + (size_t)h[10] * 2;
-            d.opw = reinterpret_cast<const double2*>(dev + bytes_i) + (size_t)h[10] * 2;
+            d.ops = reinterpret_cast<const int4*>(dev) + h[10];
+            d.lw = reinterpret_cast<const double*>(dev + off_w) + h[14];
             // level offsets index the class's op array (post offsets already
             // rebased after the body ops by the generator)
             const int* a0 = daux + h[11];
@@ -273,6 +272,8 @@ struct PairBlock {
     std::vector<int> bin;                    // reference order
     std::vector<int> sorted;                 // sorted position -> reference index (bins >= 0)
     int bin_off[17];                         // sorted pairs with bin < b start at bin_off[b]
+    std::vector<int> nuse;                   // sorted order: significant primitive pairs
+    std::vector<long long> nuse_prefix;      // sorted order: prefix sums of nuse
 };
 
 struct ClassTasks {
@@ -281,7 +282,7 @@ struct ClassTasks {
     int la = 0, lb = 0, lc = 0, ld = 0;
     std::vector<WorkItem> items;
     size_t offset = 0;
-    long long quartets = 0, prim_quartets = 0;
+    long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0;
 };
 
 struct TaskSet {
@@ -333,7 +334,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         const size_t n = sorted ? pb.sorted.size() : pb.pairs.size();
         npairs[b] = (int)n;
         const size_t k = (size_t)pb.ka * pb.kb;
-        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + 2 * n * sizeof(int);
+        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + 3 * n * sizeof(int);
         bytes = (bytes + 255) & ~size_t(255);
         offs[b + 1] = offs[b] + bytes;
     }
@@ -341,12 +342,14 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
     s->h_blocks.assign(nb, PairBlockDev{});
     const double kconst = std::sqrt(2.0 / std::sqrt(M_PI));
     for (size_t b = 0; b < nb; b++) {
+        if (sorted) s->blocks[b].nuse.assign(npairs[b], 0);
         const PairBlock& pb = s->blocks[b];
         const size_t n = npairs[b];
         const int kp = pb.ka * pb.kb;
         double* prim = reinterpret_cast<double*>(host.data() + offs[b]);
         double* ab = prim + 9 * (size_t)kp * n;
         int* ao = reinterpret_cast<int*>(ab + 3 * n);
+        int* nuse = ao + 2 * n;
         for (size_t i = 0; i < n; i++) {
             const int ref = sorted ? pb.sorted[i] : (int)i;
             const Shell& A = s->shells[pb.pairs[ref].first];
@@ -358,6 +361,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
             }
             ao[i] = A.ao0;
             ao[n + i] = B.ao0;
+            std::vector<std::array<double, 9>> vals(kp);
             for (int ka = 0; ka < pb.ka; ka++)
                 for (int kb = 0; kb < pb.kb; kb++) {
                     const int p = ka * pb.kb + kb;
@@ -365,7 +369,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
                     const double fz = M_PI / z;
                     const double sab = fz * std::sqrt(fz) * std::exp(-ea * eb / z * r2);
                     const double cab = A.c[ka] * B.c[kb] * sab;
-                    double v[9];
+                    std::array<double, 9>& v = vals[p];
                     v[0] = z;
                     v[1] = 0.5 / z;
                     v[2] = cab * std::sqrt(z) * kconst;
@@ -373,10 +377,25 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
                         v[3 + x] = (ea * A.xyz[x] + eb * B.xyz[x]) / z;
                         v[6 + x] = v[3 + x] - B.xyz[x];
                     }
-                    for (int f = 0; f < 9; f++) prim[((size_t)f * kp + p) * n + i] = v[f];
                 }
+            // significant primitive pairs first; the kernels loop over the first nuse
+            std::stable_sort(vals.begin(), vals.end(), [](const std::array<double, 9>& x,
+                                                          const std::array<double, 9>& y) {
+                return std::fabs(x[2]) > std::fabs(y[2]);
+            });
+            int used = 0;
+            while (used < kp && std::fabs(vals[used][2]) >= VLX_PRIM_CUTOFF) used++;
+            nuse[i] = std::max(used, 1);
+            if (sorted) s->blocks[b].nuse[i] = nuse[i];
+            for (int p = 0; p < kp; p++)
+                for (int f = 0; f < 9; f++) prim[((size_t)f * kp + p) * n + i] = vals[p][f];
         }
     }
+    if (sorted)
+        for (auto& pb : s->blocks) {
+            pb.nuse_prefix.assign(pb.nuse.size() + 1, 0);
+            for (size_t i = 0; i < pb.nuse.size(); i++) pb.nuse_prefix[i + 1] = pb.nuse_prefix[i] + pb.nuse[i];
+        }
     if (s->d_pairs) cudaFree(s->d_pairs);
     s->d_pairs = nullptr;
     VLX_CUDA(cudaMalloc(&s->d_pairs, host.size()));
@@ -389,6 +408,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         d.prim = reinterpret_cast<const double*>(s->d_pairs + offs[b]);
         d.ab = d.prim + 9 * (size_t)kp * n;
         d.ao = reinterpret_cast<const int*>(d.ab + 3 * n);
+        d.nuse = d.ao + 2 * n;
         d.npairs = (int)n;
         d.kprim = kp;
         d.la = pb.la;
@@ -513,10 +533,13 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                     w.kbeg = k0;
                     w.kend = k1;
                     ct.items.push_back(w);
+                    const long long evaluated =
+                        (long long)Pb.nuse[x] * (Pk.nuse_prefix[k1] - Pk.nuse_prefix[k0]);
                     ts.quartets += k1 - k0;
-                    ts.prim_quartets += (long long)(k1 - k0) * kp;
+                    ts.prim_quartets += evaluated;
                     ct.quartets += k1 - k0;
-                    ct.prim_quartets += (long long)(k1 - k0) * kp;
+                    ct.prim_quartets += evaluated;
+                    ct.ref_prim_quartets += (long long)(k1 - k0) * kp;
                 }
             }
         }

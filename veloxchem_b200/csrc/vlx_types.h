@@ -3,12 +3,20 @@
 
 #include <stdint.h>
 
-// Boys-function Chebyshev table: orders 0..BOYS_MMAX, unit intervals on
-// [0, BOYS_TMAX), BOYS_NCOEF coefficients per (order, interval).
+// Boys-function Chebyshev table: orders 0..BOYS_MMAX, intervals of width
+// 1 / BOYS_INV_H on [0, BOYS_TMAX), BOYS_NCOEF coefficients per (order,
+// interval); degree 9 on half-unit intervals keeps ~3e-15 relative accuracy.
 #define BOYS_MMAX 16
 #define BOYS_TMAX 40
-#define BOYS_NINT 40
-#define BOYS_NCOEF 14
+#define BOYS_INV_H 2
+#define BOYS_NINT (BOYS_TMAX * BOYS_INV_H)
+#define BOYS_NCOEF 10
+
+// Primitive pairs whose prefactor N_a N_b S_ab sqrt(zeta) (2/sqrt(pi))^{1/2}
+// is below this bound are skipped: their contribution to any integral is below
+// 1e-24 times the partner pair's prefactor and the recursion factors, i.e. far
+// below double-precision resolution of the contracted integrals.
+#define VLX_PRIM_CUTOFF 1e-24
 
 // Highest angular momentum per shell compiled into the class kernels.
 #define VLX_LMAX 3
@@ -18,9 +26,10 @@ namespace vlx {
 // One pair block (shell pairs of GTO blocks (la, Ka) x (lb, Kb)), pairs sorted
 // by Schwarz bin.  Arrays live in one device allocation owned by the screener.
 struct PairBlockDev {
-    const double* prim;  // [9][kprim][npairs]
+    const double* prim;  // [9][kprim][npairs], per pair sorted by |kfac| descending
     const double* ab;    // [3][npairs]  B - A
     const int* ao;       // [2][npairs]  AO index of component 0 of A and of B
+    const int* nuse;     // [npairs]     primitive pairs with |kfac| >= VLX_PRIM_CUTOFF
     int npairs;
     int kprim;
     int la, lb;
