@@ -158,6 +158,21 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_den
  * (src/t4c_func/FockDriver.cpp:76-117). */
 int vlx_b200_compute_eri(vlx_b200_screener* screener, int ithreshold, double* eri_out);
 
+/* One-electron matrix between a bra basis and a ket basis of one molecule
+ * (the same shell tables for the ordinary matrices; a minimal bra basis for
+ * the mixed overlap of the SAD guess): which = 0 overlap S, 1 kinetic energy
+ * T, 2 nuclear attraction V = -sum_C Z_C <a| 1/|r - C| |b>.  Shell tables as
+ * for vlx_b200_screener_create (raw coefficients); Z: nuclear charges; out:
+ * host nao_bra x nao_ket, row-major, reference AO order.
+ * Replaces COverlapDriver::compute (src/t2c_overlap/OverlapDriver.hpp:50-57),
+ * CKineticEnergyDriver::compute (src/t2c_kinetic_energy/KineticEnergyDriver.hpp)
+ * and CNuclearPotentialDriver::compute negated as
+ * compute_nuclear_potential_integrals does (src/pymodule/oneeints.py:71-95). */
+int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                          const int* bra_atom, const int* bra_l, const int* bra_nprim, const double* bra_exps,
+                          const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
+                          const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out);
+
 /* Boys function F_m(T) for n arguments as the device evaluates it
  * (host arrays T[n] in, F[n] out), for validation. */
 int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F);

@@ -75,6 +75,8 @@ class RefOracle:
                                               ctypes.POINTER(ctypes.c_char_p), ctypes.c_double, ctypes.c_double,
                                               ctypes.c_int, _dp]
             lib.vlxref_eri.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+            lib.vlxref_one_electron.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+            lib.vlxref_overlap_mixed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp]
             cls._lib = lib
         return cls._lib
 
@@ -130,6 +132,18 @@ class RefOracle:
     def eri(self, ithreshold=12):
         out = np.zeros((self.nao,) * 4)
         self.lib().vlxref_eri(self._h, int(ithreshold), _d(out))
+        return out
+
+    def one_electron(self, which):
+        """0 = overlap S, 1 = kinetic T, 2 = nuclear attraction V (negative)."""
+        out = np.zeros((self.nao, self.nao))
+        self.lib().vlxref_one_electron(self._h, int(which), _d(out))
+        return out
+
+    def overlap_mixed(self, other):
+        """Overlap between this system's basis (rows) and other's basis (columns)."""
+        out = np.zeros((self.nao, other.nao))
+        self.lib().vlxref_overlap_mixed(self._h, other._h, _d(out))
         return out
 
 

@@ -10,7 +10,10 @@
 //   * Matrix.set_values / full_matrix as in src/python/ExportMath.cpp:258-305,
 //   * _FockDriver._compute_fock_omp / _compute_local_fock / compute_eri as in
 //     src/python/ExportT4CIntegrals.cpp:48-124,
-//   * T4CScreener.partition as in src/t4c_func/T4CScreener.cpp:63-119.
+//   * T4CScreener.partition as in src/t4c_func/T4CScreener.cpp:63-119,
+//   * one-electron integrals: COverlapDriver, CKineticEnergyDriver and
+//     CNuclearPotentialDriver (negated as compute_nuclear_potential_integrals
+//     does, src/pymodule/oneeints.py:71-95).
 
 #include <omp.h>
 
@@ -23,6 +26,9 @@
 #include "BlockedGtoPairBlock.hpp"
 #include "Dense4DTensor.hpp"
 #include "FockDriver.hpp"
+#include "KineticEnergyDriver.hpp"
+#include "NuclearPotentialDriver.hpp"
+#include "OverlapDriver.hpp"
 #include "GtoPairBlock.hpp"
 #include "Matrices.hpp"
 #include "Matrix.hpp"
@@ -272,6 +278,35 @@ vlxref_eri(void* handle, const int ithreshold, double* eri_out)
     const auto t   = drv.compute_eri(sys->screener, sys->nao, ithreshold);
     const size_t n = static_cast<size_t>(sys->nao);
     std::memcpy(eri_out, t.values(), sizeof(double) * n * n * n * n);
+    return 0;
+}
+
+// Overlap S, kinetic T and nuclear attraction V (= -sum_C Z_C <a|1/r_C|b>)
+// in the full-matrix AO order; which: 0 = S, 1 = T, 2 = V.
+int
+vlxref_one_electron(void* handle, const int which, double* out)
+{
+    auto sys = static_cast<RefSystem*>(handle);
+    CMatrix m;
+    if (which == 0) m = COverlapDriver().compute(sys->basis, sys->molecule);
+    else if (which == 1) m = CKineticEnergyDriver().compute(sys->basis, sys->molecule);
+    else m = CNuclearPotentialDriver().compute(sys->basis, sys->molecule);
+    const auto full = m.full_matrix();
+    const size_t n = static_cast<size_t>(sys->nao);
+    for (size_t i = 0; i < n * n; i++) out[i] = (which == 2 ? -1.0 : 1.0) * full.data()[i];
+    return 0;
+}
+
+// Overlap between the basis of `bra` and the basis of `ket` (same molecule),
+// nao(bra) x nao(ket), as the SAD guess uses it.
+int
+vlxref_overlap_mixed(void* bra, void* ket, double* out)
+{
+    auto a = static_cast<RefSystem*>(bra);
+    auto b = static_cast<RefSystem*>(ket);
+    const auto m    = COverlapDriver().compute(a->basis, b->basis, a->molecule);
+    const auto full = m.full_matrix();
+    std::memcpy(out, full.data(), sizeof(double) * a->nao * b->nao);
     return 0;
 }
 

@@ -1,0 +1,117 @@
+"""One-electron integrals and the restricted HF SCF.
+
+Pins: the reference's own overlap / kinetic / nuclear-attraction drivers
+(compiled into oracle/_ref) and the reference's SCF energy known answer for the
+water dimer / def2-SVP, -151.9220860932 Eh to 1e-8 (tests/test_scf_rest.py of
+the reference, geometry from the same test)."""
+
+import numpy as np
+import pytest
+
+from oracle.oracle import ref_available
+
+REF_ENERGY = -151.9220860932
+
+DIMER_XYZ = """
+O   -0.1858140  -1.1749469   0.7662596
+H   -0.1285513  -0.8984365   1.6808606
+H   -0.0582782  -0.3702550   0.2638279
+O    0.1747051  11.1050002  -0.7244430
+H   -0.5650842  11.3134964  -1.2949455
+H    0.9282185  11.0652990  -1.3134026
+"""
+
+
+def _dimer(basis='def2-svp'):
+    from veloxchem_b200 import MolecularBasis, Molecule
+    mol = Molecule.read_str(DIMER_XYZ)
+    return mol, MolecularBasis.read(mol, basis)
+
+
+@pytest.mark.skipif(not ref_available(), reason='reference oracle not built')
+def test_cpu_scf_restatement_reaches_reference_energy():
+    """A plain numpy SCF over the compiled reference (S, T, V, FockDriver):
+    pins the energy expression and the orthogonalisation used by the driver."""
+    from oracle.oracle import RefOracle
+    mol, bas = _dimer()
+    ref = RefOracle(mol, bas)
+    S, T, V = ref.one_electron(0), ref.one_electron(1), ref.one_electron(2)
+    H = T + V
+    w, u = np.linalg.eigh(S)
+    X = u[:, w > 1e-6] / np.sqrt(w[w > 1e-6])
+    nocc = mol.number_of_electrons() // 2
+    e, c = np.linalg.eigh(X.T @ H @ X)
+    D = X @ c[:, :nocc] @ (X @ c[:, :nocc]).T
+    focks, errs, energy = [], [], 0.0
+    for _ in range(60):
+        F2 = ref.fock(D, '2jk', 1.0, 0.0, 12)
+        energy = np.sum(D * F2) + 2 * np.sum(D * H) + mol.nuclear_repulsion_energy()
+        F = F2 + H
+        err = X.T @ (F @ D @ S - S @ D @ F) @ X
+        if 2 * np.linalg.norm(err) < 1e-7:
+            break
+        focks.append(F)
+        errs.append(err)
+        n = len(focks)
+        B = -np.ones((n + 1, n + 1))
+        B[n, n] = 0
+        for i in range(n):
+            for j in range(n):
+                B[i, j] = np.sum(errs[i] * errs[j])
+        rhs = np.zeros(n + 1)
+        rhs[n] = -1
+        coef = np.linalg.lstsq(B, rhs, rcond=None)[0]
+        Fe = sum(cf * f for cf, f in zip(coef[:n], focks))
+        e, c = np.linalg.eigh(X.T @ Fe @ X)
+        D = X @ c[:, :nocc] @ (X @ c[:, :nocc]).T
+    assert abs(energy - REF_ENERGY) < 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('basis', ['def2-svpd', 'def2-tzvp'])
+def test_one_electron_against_reference(basis):
+    from conftest import load_golden
+    from oracle.oracle import RefOracle
+    from veloxchem_b200 import _native as nat
+    name = 'h2o_dimer_svpd.npz' if basis == 'def2-svpd' else 'h2o_dimer_tzvp.npz'
+    g, mol, bas = load_golden(name)
+    ref = RefOracle(mol, bas, partition=False)
+    for which in range(3):
+        assert np.max(np.abs(nat.one_electron(which, mol, bas) - ref.one_electron(which))) < 1e-11, which
+
+
+@pytest.mark.gpu
+def test_mixed_overlap_against_reference():
+    from oracle.oracle import RefOracle
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200 import _native as nat
+    mol, bas = _dimer()
+    mini = MolecularBasis.read(mol, 'ao-start-guess')
+    ref = RefOracle(mol, mini, partition=False).overlap_mixed(RefOracle(mol, bas, partition=False))
+    assert np.max(np.abs(nat.one_electron(0, mol, mini, bas) - ref)) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('guess', ['sad', 'core'])
+def test_scf_energy_known_answer(guess):
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol, bas = _dimer()
+    drv = ScfRestrictedDriver()
+    drv.guess = guess
+    res = drv.compute(mol, bas)
+    assert res['converged']
+    assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
+
+
+@pytest.mark.gpu
+def test_sad_density_is_a_valid_guess():
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200 import _native as nat
+    from veloxchem_b200.scf import SadGuessDriver
+    mol, bas = _dimer()
+    mini = MolecularBasis.read(mol, 'ao-start-guess')
+    D = SadGuessDriver().compute(mol, mini, bas)
+    S = nat.one_electron(0, mol, bas)
+    # trace(D S) = number of alpha electrons of the neutral atoms
+    assert abs(np.trace(D @ S) - mol.number_of_electrons() / 2) < 1e-10
+    assert np.allclose(D, D.T)

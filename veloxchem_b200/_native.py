@@ -44,6 +44,8 @@ SIGNATURES = {
     'vlx_b200_fock_profile': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double, ctypes.c_int,
                                              _vp, _vp, ctypes.c_int, _vp, _ip]),
     'vlx_b200_fp64_peak': (ctypes.c_int, [ctypes.c_int, _dp]),
+    'vlx_b200_one_electron': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int,
+                                             _ip, _ip, _ip, _dp, _dp, ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]),
     'vlx_b200_fock_build_noalloc': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_int, _vp, _vp]),
 }
@@ -138,6 +140,20 @@ def normalize_shell(l, exps, coefs):
     c = f64(coefs).copy()
     check(lib().vlx_b200_normalize_shell(int(l), len(e), dptr(e), dptr(c)), 'normalize_shell')
     return c
+
+
+def one_electron(which, molecule, bra_basis, ket_basis=None, device=0):
+    """S (which=0), T (1) or V (2) between bra_basis and ket_basis (default: bra)."""
+    ket_basis = bra_basis if ket_basis is None else ket_basis
+    z = i32(molecule.get_element_ids())
+    xyz = f64(molecule.get_coordinates_in_bohr())
+    ba, bl, bn, be, bc = [a if a.dtype == np.float64 else i32(a) for a in bra_basis.shell_table()]
+    ka, kl, kn, ke, kc = [a if a.dtype == np.float64 else i32(a) for a in ket_basis.shell_table()]
+    out = np.zeros((bra_basis.get_dimensions_of_basis(), ket_basis.get_dimensions_of_basis()))
+    check(lib().vlx_b200_one_electron(int(device), int(which), len(z), iptr(z), dptr(xyz), len(ba), iptr(ba),
+                                      iptr(bl), iptr(bn), dptr(f64(be)), dptr(f64(bc)), len(ka), iptr(ka), iptr(kl),
+                                      iptr(kn), dptr(f64(ke)), dptr(f64(kc)), dptr(out)), 'one_electron')
+    return out
 
 
 def boys_device(m, t, device=0):

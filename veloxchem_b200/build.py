@@ -36,7 +36,8 @@ def nvcc():
 
 def _headers_digest():
     h = hashlib.sha256()
-    for p in sorted(list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) + [GEN / 'dispatch.inc', INCLUDE / 'vlx_b200.h']):
+    for p in sorted(list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) +
+                    [GEN / 'dispatch.inc', GEN / 'sph_table.inc', INCLUDE / 'vlx_b200.h']):
         if p.exists():
             h.update(p.read_bytes())
     h.update(' '.join(NVCC_FLAGS).encode())
@@ -74,7 +75,7 @@ def build(jobs=None, lmax=3, verbose=True):
     if not asm.exists() or asm.read_text() != asm_text:
         asm.write_text(asm_text)
     hdr = _headers_digest()
-    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_host.cu']
+    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_onee.cu', CSRC / 'vlx_host.cu']
     objs = [OBJ / (s.stem + '.o') for s in sources]
     jobs = jobs or os.cpu_count() or 4
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:

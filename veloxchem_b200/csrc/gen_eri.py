@@ -601,6 +601,23 @@ def emit_dispatch(compiled, lmax, outdir):
         path.write_text(text)
 
 
+def emit_sph_table(outdir, lmax=4):
+    """Spherical factors for l <= lmax as a constant table [l][m][cart]
+    (m = 0..2l for -l..l, lexicographic Cartesian components)."""
+    vals = []
+    for l in range(lmax + 1):
+        rows = sph_coefficients(l)
+        for m in range(9):
+            for c in range(15):
+                vals.append(rows[m][c] if (m < 2 * l + 1 and c < ncart(l)) else 0.0)
+    text = ('// Generated by gen_eri.py -- do not edit.\n#pragma once\n'
+            '#define VLX_SPH_LMAX %d\n' % lmax +
+            '__constant__ double c_sph[%d] = {%s};\n' % (len(vals), ', '.join(repr(v) for v in vals)))
+    path = outdir / 'sph_table.inc'
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+
+
 def main():
     outdir = Path(sys.argv[1])
     lmax = int(sys.argv[2]) if len(sys.argv) > 2 else 3
@@ -614,6 +631,7 @@ def main():
     for cls in compiled:
         emit_class_file(cls, outdir)
     emit_dispatch(compiled, lmax, outdir)
+    emit_sph_table(outdir)
     import gen_coop
     gen_coop.emit_blob(interp, outdir / 'coop_programs.bin')
     for p in outdir.glob('class_*.cu'):

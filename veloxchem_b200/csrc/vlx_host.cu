@@ -34,6 +34,22 @@
 extern "C" const char vlx_coop_blob_start[];
 extern "C" const char vlx_coop_blob_end[];
 
+namespace vlx {
+struct OneShellSet {
+    const double* xyz;
+    const int* l;
+    const int* nprim;
+    const int* poff;
+    const int* ao0;
+    const int* nl;
+    const double* exps;
+    const double* coefs;
+    int nshells;
+};
+void launch_one_electron(int which, const OneShellSet& bra, const OneShellSet& ket, int natoms, const double* zc,
+                         const double* cxyz, const double* boys, double* out, int nao_ket, cudaStream_t st);
+}  // namespace vlx
+
 using vlx::FockArgs;
 using vlx::CoopClassDev;
 using vlx::PairBlockDev;
@@ -1084,6 +1100,106 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
         VLX_CUDA(cudaMemcpyAsync(d_fock, sc.acc, bytes, cudaMemcpyDeviceToDevice, st));
     }
     return VLX_B200_OK;
+}
+
+int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                          const int* bra_atom, const int* bra_l, const int* bra_nprim, const double* bra_exps,
+                          const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
+                          const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out)
+{
+    if (which < 0 || which > 2 || natoms < 1 || !Z || !xyz || nsh_bra < 1 || nsh_ket < 1 || !out)
+        return fail(VLX_B200_ERR_ARGUMENT, "one_electron: invalid arguments");
+    DeviceGlobals* g = nullptr;
+    int rc = device_globals(device, &g);
+    if (rc) return rc;
+    VLX_CUDA(cudaSetDevice(device));
+    // host shell sets: normalised primitive factors, AO map of each basis
+    struct HostSet {
+        std::vector<double> xyz, exps, coefs;
+        std::vector<int> l, nprim, poff, ao0, nl;
+        int nao = 0;
+    };
+    auto make = [&](int nsh, const int* atom, const int* lv, const int* np, const double* e, const double* c,
+                    HostSet& h) -> int {
+        h.nl.assign(VLX_LMAX + 1, 0);
+        size_t off = 0;
+        for (int i = 0; i < nsh; i++) {
+            if (lv[i] < 0 || lv[i] > VLX_LMAX || np[i] < 1 || atom[i] < 0 || atom[i] >= natoms)
+                return fail(VLX_B200_ERR_ARGUMENT, "one_electron: invalid shell table");
+            h.l.push_back(lv[i]);
+            h.nprim.push_back(np[i]);
+            h.poff.push_back((int)off);
+            for (int x = 0; x < 3; x++) h.xyz.push_back(xyz[3 * atom[i] + x]);
+            std::vector<double> cc(c + off, c + off + np[i]);
+            normalize_shell(lv[i], np[i], e + off, cc.data());
+            for (int k = 0; k < np[i]; k++) {
+                h.exps.push_back(e[off + k]);
+                h.coefs.push_back(cc[k]);
+            }
+            off += np[i];
+            h.nl[lv[i]]++;
+        }
+        int loff[VLX_LMAX + 2] = {0}, cnt[VLX_LMAX + 1] = {0};
+        for (int l = 0; l <= VLX_LMAX; l++) loff[l + 1] = loff[l] + h.nl[l] * (2 * l + 1);
+        h.nao = loff[VLX_LMAX + 1];
+        for (int i = 0; i < nsh; i++) h.ao0.push_back(loff[h.l[i]] + cnt[h.l[i]]++);
+        return VLX_B200_OK;
+    };
+    HostSet hb, hk;
+    rc = make(nsh_bra, bra_atom, bra_l, bra_nprim, bra_exps, bra_coefs, hb);
+    if (rc) return rc;
+    rc = make(nsh_ket, ket_atom, ket_l, ket_nprim, ket_exps, ket_coefs, hk);
+    if (rc) return rc;
+    std::vector<double> zc(natoms);
+    for (int a = 0; a < natoms; a++) zc[a] = Z[a];
+    // one device buffer for everything
+    std::vector<void*> bufs;
+    auto up = [&](const void* src, size_t bytes, void** dst) -> int {
+        VLX_CUDA(cudaMalloc(dst, std::max<size_t>(bytes, 8)));
+        bufs.push_back(*dst);
+        if (bytes) VLX_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return VLX_B200_OK;
+    };
+    auto free_all = [&]() {
+        for (void* b : bufs) cudaFree(b);
+    };
+    vlx::OneShellSet sets[2];
+    HostSet* hs[2] = {&hb, &hk};
+    for (int k = 0; k < 2 && !rc; k++) {
+        HostSet& h = *hs[k];
+        void *dx, *dl, *dn, *dp, *da, *dnl, *de, *dc;
+        rc = up(h.xyz.data(), h.xyz.size() * 8, &dx);
+        if (!rc) rc = up(h.l.data(), h.l.size() * 4, &dl);
+        if (!rc) rc = up(h.nprim.data(), h.nprim.size() * 4, &dn);
+        if (!rc) rc = up(h.poff.data(), h.poff.size() * 4, &dp);
+        if (!rc) rc = up(h.ao0.data(), h.ao0.size() * 4, &da);
+        if (!rc) rc = up(h.nl.data(), h.nl.size() * 4, &dnl);
+        if (!rc) rc = up(h.exps.data(), h.exps.size() * 8, &de);
+        if (!rc) rc = up(h.coefs.data(), h.coefs.size() * 8, &dc);
+        if (rc) break;
+        sets[k] = {static_cast<const double*>(dx), static_cast<const int*>(dl), static_cast<const int*>(dn),
+                   static_cast<const int*>(dp), static_cast<const int*>(da), static_cast<const int*>(dnl),
+                   static_cast<const double*>(de), static_cast<const double*>(dc), (int)h.l.size()};
+    }
+    void *dz = nullptr, *dxyz = nullptr, *dout = nullptr;
+    if (!rc) rc = up(zc.data(), zc.size() * 8, &dz);
+    if (!rc) rc = up(xyz, (size_t)natoms * 3 * 8, &dxyz);
+    const size_t obytes = (size_t)hb.nao * hk.nao * sizeof(double);
+    if (!rc) {
+        cudaError_t e = cudaMalloc(&dout, obytes);
+        if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+        else bufs.push_back(dout);
+    }
+    if (!rc) {
+        cudaMemset(dout, 0, obytes);
+        vlx::launch_one_electron(which, sets[0], sets[1], natoms, static_cast<const double*>(dz),
+                                 static_cast<const double*>(dxyz), g->boys, static_cast<double*>(dout), hk.nao, 0);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(out, dout, obytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, std::string("one_electron: ") + cudaGetErrorString(e));
+    }
+    free_all();
+    return rc;
 }
 
 int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)

@@ -1,0 +1,223 @@
+"""Restricted closed-shell Hartree-Fock on the GPU around the B200 Fock build.
+
+Mirrors the reference's ScfRestrictedDriver (src/pymodule/scfdriver.py,
+scfrestdriver.py) for the parts a restricted HF energy needs:
+
+* one-electron matrices S, T, V from ``vlx_b200_one_electron`` (reference:
+  ScfDriver._comp_one_ints, scfdriver.py:1252, 1700-1781);
+* canonical orthogonalisation X = U_k / sqrt(s_k) over eigenvalues of S above
+  ``ovl_thresh`` = 1e-6 (scfdriver.py:1280-1300);
+* initial density: SAD (SadGuessDriver.compute, sadguessdriver.py:841-971)
+  built from the minimal basis ``ao-start-guess`` with neutral-atom occupation
+  numbers (the reference also shifts them by dftd4/EEQ partial charges), or
+  the core-Hamiltonian guess;
+* per iteration: F_2e = 2J - K from the device-resident Fock build with the
+  reference's dynamic integral threshold (_get_dyn_threshold,
+  scfdriver.py:2410-2435), energy terms e_ee = sum D F_2e, e_kin = 2 sum D T,
+  e_en = 2 sum D V (scfdriver.py:2115-2171), F = F_2e + T + V
+  (scfdriver.py:2173-2215), electronic gradient
+  2 ||X^T (F D S - S D F) X|| (scfrestdriver.py:70-107), Pulay DIIS on the
+  commutator (the reference uses C2-DIIS, c2diis.py), MOs from X^T F X and
+  D = C_occ C_occ^T (scfrestdriver.py:214-269);
+* convergence when the electronic gradient is below ``conv_thresh``
+  (default 1e-6, scfdriver.py:151).
+
+Linear algebra runs in FP64 with torch on the same GPU; the Fock build is the
+native library's.
+"""
+
+import ctypes
+import math
+import time
+
+import numpy as np
+
+from . import _native as nat
+from .molecularbasis import MolecularBasis
+from .screener import T4CScreener
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class SadGuessDriver:
+    """Superposition of atomic densities in the minimal basis ``ao-start-guess``,
+    projected onto the AO basis (reference SadGuessDriver.compute)."""
+
+    @staticmethod
+    def occupation_numbers(elem_id, nelec=0.0):
+        """Alpha occupation of the minimal-basis functions of a neutral atom
+        (reference get_occupation_numbers_for_element, H..Ne)."""
+        if elem_id == 1:
+            return [max(0.0, 0.5 + nelec)]
+        if elem_id == 2:
+            return [max(0.0, 1.0 + nelec)]
+        if elem_id in (3, 4):
+            return [1.0, max(0.0, 0.5 * (elem_id - 2) + nelec)]
+        if 5 <= elem_id <= 10:
+            occ = max(0.0, 0.125 * (elem_id - 2) + nelec / 4.0)
+            return [1.0, occ, occ, occ, occ]
+        raise ValueError('SAD occupations implemented for H..Ne only')
+
+    @staticmethod
+    def ao_indices_of_atoms(molecule, basis):
+        natoms = molecule.number_of_atoms()
+        idx = [[] for _ in range(natoms)]
+        ao = 0
+        for l in range(basis.max_angular_momentum() + 1):
+            for _m in range(2 * l + 1):
+                for a in range(natoms):
+                    for s in basis.shells:
+                        if s.atom == a and s.l == l:
+                            idx[a].append(ao)
+                            ao += 1
+        return idx
+
+    def compute(self, molecule, min_basis, ao_basis, device=0):
+        s12 = nat.one_electron(0, molecule, min_basis, ao_basis, device)
+        s22 = nat.one_electron(0, molecule, ao_basis, None, device)
+        ao1 = self.ao_indices_of_atoms(molecule, min_basis)
+        ao2 = self.ao_indices_of_atoms(molecule, ao_basis)
+        csad = np.zeros((s22.shape[0], s12.shape[0]))
+        for a, z in enumerate(molecule.get_element_ids()):
+            i1, i2 = ao1[a], ao2[a]
+            occ = np.array(self.occupation_numbers(int(z)))
+            if len(occ) != len(i1):
+                raise ValueError('SAD: minimal basis / occupation mismatch for element %d' % z)
+            b12 = s12[np.ix_(i1, i2)]
+            b22 = s22[np.ix_(i2, i2)]
+            w, v = np.linalg.eigh(b22)
+            b22_inv = (v / w) @ v.T
+            mat_a = b12.T
+            mat_m = mat_a.T @ b22_inv @ mat_a
+            w, v = np.linalg.eigh(mat_m)
+            m_invsqrt = (v / np.sqrt(w)) @ v.T
+            c2 = b22_inv @ mat_a @ m_invsqrt
+            csad[np.ix_(i2, i1)] = c2 * np.sqrt(occ)[None, :]
+        return csad @ csad.T
+
+
+class ScfRestrictedDriver:
+    """Restricted Hartree-Fock with the B200 Fock build."""
+
+    def __init__(self, device=0):
+        self.device = int(device)
+        self.conv_thresh = 1.0e-6
+        self.max_iter = 50
+        self.max_err_vecs = 10
+        self.eri_thresh = 1.0e-12
+        self.ovl_thresh = 1.0e-6
+        self.guess = 'sad'
+        self.history = []
+        self.timings = {}
+
+    # reference ScfDriver._get_dyn_threshold
+    def dyn_threshold(self, e_grad):
+        if e_grad < 1.0e-6:
+            return self.eri_thresh
+        nteri = 1.0e-10 * math.pow(10, math.floor(math.log10(e_grad)))
+        if nteri > 1.0e-10:
+            return 1.0e-10
+        if nteri < self.eri_thresh:
+            return self.eri_thresh
+        return nteri
+
+    def compute(self, molecule, ao_basis, min_basis=None, guess_density=None, screener=None):
+        torch = _torch()
+        dev = torch.device('cuda', self.device)
+        t_start = time.perf_counter()
+        nelec = molecule.number_of_electrons()
+        if nelec % 2:
+            raise ValueError('ScfRestrictedDriver: odd number of electrons')
+        nocc = nelec // 2
+        t0 = time.perf_counter()
+        S = torch.from_numpy(nat.one_electron(0, molecule, ao_basis, None, self.device)).to(dev)
+        T = torch.from_numpy(nat.one_electron(1, molecule, ao_basis, None, self.device)).to(dev)
+        V = torch.from_numpy(nat.one_electron(2, molecule, ao_basis, None, self.device)).to(dev)
+        H = T + V
+        self.timings['one_electron_s'] = time.perf_counter() - t0
+        w, u = torch.linalg.eigh(S)
+        keep = w > self.ovl_thresh
+        X = u[:, keep] / torch.sqrt(w[keep])[None, :]
+        e_nuc = molecule.nuclear_repulsion_energy()
+        if screener is None:
+            t0 = time.perf_counter()
+            screener = T4CScreener(device=self.device)
+            screener.partition(ao_basis, molecule, 'eri')
+            self.timings['screener_s'] = time.perf_counter() - t0
+        if guess_density is not None:
+            D = torch.as_tensor(np.asarray(guess_density), dtype=torch.float64, device=dev)
+        elif self.guess == 'sad':
+            if min_basis is None:
+                min_basis = MolecularBasis.read(molecule, 'ao-start-guess')
+            D = torch.from_numpy(SadGuessDriver().compute(molecule, min_basis, ao_basis, self.device)).to(dev)
+        else:
+            e, c = torch.linalg.eigh(X.T @ H @ X)
+            C = X @ c[:, :nocc]
+            D = C @ C.T
+        stream = torch.cuda.current_stream(dev)
+        F2e = torch.empty_like(D)
+        focks, errs = [], []
+        e_grad, energy, e_old = 1.0, 0.0, 0.0
+        self.history = []
+        converged = False
+        fock_ms = 0.0
+        for it in range(1, self.max_iter + 1):
+            ith = int(-math.log10(self.dyn_threshold(e_grad)))
+            D = 0.5 * (D + D.T).contiguous()
+            t0 = time.perf_counter()
+            nat.check(nat.lib().vlx_b200_fock_build_device(screener.handle, ctypes.c_void_p(D.data_ptr()), 1, b'2jk',
+                                                            1.0, 0.0, ith, ctypes.c_void_p(F2e.data_ptr()),
+                                                            ctypes.c_void_p(stream.cuda_stream)), 'fock_build')
+            torch.cuda.synchronize(dev)
+            fock_ms += 1e3 * (time.perf_counter() - t0)
+            e_ee = torch.sum(D * F2e)
+            e_one = 2.0 * torch.sum(D * H)
+            F = F2e + H
+            energy = float(e_ee + e_one) + e_nuc
+            fds = F @ D @ S
+            err = X.T @ (fds - fds.T) @ X
+            e_grad = 2.0 * float(torch.linalg.norm(err))
+            self.history.append({'iteration': it, 'energy': energy, 'delta_e': energy - e_old, 'e_grad': e_grad,
+                                 'ithreshold': ith, 'time_s': time.perf_counter() - t_start})
+            e_old = energy
+            if e_grad < self.conv_thresh:
+                converged = True
+                break
+            focks.append(F)
+            errs.append(err)
+            if len(focks) > self.max_err_vecs:
+                focks.pop(0)
+                errs.pop(0)
+            F_eff = self._diis(focks, errs) if len(focks) > 1 else F
+            e, c = torch.linalg.eigh(X.T @ F_eff @ X)
+            C = X @ c[:, :nocc]
+            D = C @ C.T
+        self.timings['fock_ms_total'] = fock_ms
+        self.timings['total_s'] = time.perf_counter() - t_start
+        e, c = torch.linalg.eigh(X.T @ F @ X)
+        return {'scf_energy': energy, 'converged': converged, 'iterations': len(self.history),
+                'e_grad': e_grad, 'nuclear_repulsion': e_nuc, 'D_alpha': D.cpu().numpy(),
+                'C_alpha': (X @ c).cpu().numpy(), 'E_alpha': e.cpu().numpy(), 'F_alpha': F.cpu().numpy(),
+                'history': self.history, 'timings': dict(self.timings), 'screener': screener}
+
+    @staticmethod
+    def _diis(focks, errs):
+        torch = _torch()
+        n = len(focks)
+        B = torch.empty((n + 1, n + 1), dtype=torch.float64, device=focks[0].device)
+        for i in range(n):
+            for j in range(i, n):
+                B[i, j] = B[j, i] = torch.sum(errs[i] * errs[j])
+        B[n, :] = -1.0
+        B[:, n] = -1.0
+        B[n, n] = 0.0
+        rhs = torch.zeros(n + 1, dtype=torch.float64, device=focks[0].device)
+        rhs[n] = -1.0
+        coef = torch.linalg.lstsq(B.cpu(), rhs.cpu().unsqueeze(1)).solution.squeeze(1).to(focks[0].device)
+        out = torch.zeros_like(focks[0])
+        for i in range(n):
+            out += coef[i] * focks[i]
+        return out
