@@ -152,6 +152,15 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_den
                                 const char* label, double exchange_factor, double omega, int ithreshold,
                                 double* d_fock, void* stream);
 
+/* Mixed precision for the following builds of this screener: shell quartets
+ * whose Schwarz bound sqrt((ab|ab)) sqrt((cd|cd)) times max_abs_density is
+ * below `cutoff` (decided on the decade bins: bound <= 10^-(bin_ab + bin_cd))
+ * are evaluated with the FP32 recursion; digestion and the Fock accumulator
+ * stay FP64.  Classes served by the warp-cooperative kernel stay FP64.
+ * cutoff <= 0 switches it off (the default).  No counterpart in the
+ * reference (its Fock build is FP64 throughout). */
+int vlx_b200_set_fp32_threshold(vlx_b200_screener* screener, double cutoff, double max_abs_density);
+
 /* Dense (nao)^4 ERI tensor over the screened unique quartets (all eight
  * index permutations written), host buffer.
  * Replaces CFockDriver::compute_eri(screener, nao, ithreshold)
@@ -184,7 +193,8 @@ typedef struct {
     double device_ms;          /* CUDA-event duration of the class launch */
     long long shell_quartets;  /* unique shell quartets in the launch */
     long long prim_quartets;   /* primitive quartets in the launch */
-    double flops;              /* algorithmic FP64 flops of the launch */
+    double flops;              /* algorithmic flops of the launch */
+    long long fp32_quartets;   /* of shell_quartets, evaluated in FP32 (mixed precision) */
 } vlx_b200_class_profile;
 
 /* A device-resident build (as vlx_b200_fock_build_device, ithreshold and

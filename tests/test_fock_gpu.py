@@ -203,3 +203,44 @@ def test_large_cluster_properties():
     k1 = _fock(s, d1, 'k', 1.0, 12)
     f1 = _fock(s, d1, '2jk', 1.0, 12)
     assert np.max(np.abs(f1 - (2 * j1 - k1))) < 1e-9
+
+
+def test_mixed_precision_build():
+    """FP32 for quartets with bound x max|D| below the cutoff: no FP32 quartet
+    at a vanishing cutoff (bitwise the FP64 path), a bounded Fock error and a
+    real FP32 share at the default cutoffs; switching off restores FP64."""
+    import torch
+    from veloxchem_b200 import _native as nat
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    d = torch.from_numpy(g['density']).cuda()
+    f64 = torch.empty_like(d)
+    prof64 = nat.fock_profile(s, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
+    assert sum(p['fp32_quartets'] for p in prof64) == 0
+    dmax = float(d.abs().max())
+    errors = {}
+    for cutoff in (1e-9, 1e-7, 1e-5):
+        s.set_fp32_threshold(cutoff, dmax)
+        fm = torch.empty_like(d)
+        prof = nat.fock_profile(s, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
+        n32 = sum(p['fp32_quartets'] for p in prof)
+        assert n32 > 0
+        errors[cutoff] = float((fm - f64).abs().max())
+    assert errors[1e-9] < 1e-10 and errors[1e-7] < 1e-8 and errors[1e-5] < 1e-6
+    s.set_fp32_threshold(0.0, 0.0)
+    f2 = torch.empty_like(d)
+    nat.fock_profile(s, d.data_ptr(), f2.data_ptr(), '2jk', 1.0, 12)
+    assert float((f2 - f64).abs().max()) < 1e-12
+
+
+def test_mixed_precision_scf_energy():
+    """SCF with FP32 small quartets until the gradient is below 1e-4 reaches the
+    FP64 energy (the final iterations are FP64)."""
+    from test_scf import REF_ENERGY, _dimer
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol, bas = _dimer()
+    drv = ScfRestrictedDriver()
+    drv.fp32_cutoff = 1e-6
+    res = drv.compute(mol, bas)
+    assert res['converged'] and any(h['mixed'] for h in res['history'])
+    assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8

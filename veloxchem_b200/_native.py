@@ -46,6 +46,7 @@ SIGNATURES = {
     'vlx_b200_fp64_peak': (ctypes.c_int, [ctypes.c_int, _dp]),
     'vlx_b200_one_electron': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int,
                                              _ip, _ip, _ip, _dp, _dp, ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]),
+    'vlx_b200_set_fp32_threshold': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     'vlx_b200_fock_build_noalloc': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_int, _vp, _vp]),
 }
@@ -55,7 +56,7 @@ class ClassProfile(ctypes.Structure):
     _fields_ = [('la', ctypes.c_int), ('lb', ctypes.c_int), ('lc', ctypes.c_int), ('ld', ctypes.c_int),
                 ('table_driven', ctypes.c_int), ('device_ms', ctypes.c_double),
                 ('shell_quartets', ctypes.c_longlong), ('prim_quartets', ctypes.c_longlong),
-                ('flops', ctypes.c_double)]
+                ('flops', ctypes.c_double), ('fp32_quartets', ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

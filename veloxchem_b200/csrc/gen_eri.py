@@ -25,6 +25,7 @@ Usage: python gen_eri.py OUTDIR [LMAX]
 """
 
 import math
+import re
 import sys
 from pathlib import Path
 
@@ -202,6 +203,7 @@ class ClassGen:
           % (la, lb, lc, ld, len(self.vrr.order), len(e_t) * len(f_t), nsph))
         w('template <> struct EriClass<%d, %d, %d, %d> {' % (la, lb, lc, ld))
         w('    static constexpr int NSPH = %d;' % nsph)
+        method_start = len(lines)
         w('    template <class BraT, class KetT>')
         w('    __device__ __forceinline__ static void compute(const BraT& bra, const KetT& ket, const double* __restrict__ btab,')
         w('                                                   double* __restrict__ out)')
@@ -335,6 +337,8 @@ class ClassGen:
                                 terms.append('%s * %s' % (_num(sph_a[i][ia] * sph_b[j][jb]), names[(a, b)]))
                         w('        out[%d] = %s;' % (((i * nb + j) * nc + k) * nd + l, ' + '.join(terms)))
         w('    }')
+        body = lines[method_start:]
+        lines.extend(to_f32(body))
         w('};')
         return '\n'.join(lines)
 
@@ -490,6 +494,26 @@ class ClassGen:
         acc_first = min(acc_slot.values())
         return dict(nslots=nxt[0], vrr=vrr_ops, acc=acc_ops, post=post, out=out_slots,
                     acc_first=acc_first, nacc=len(acc_ops))
+
+_FLOAT_LITERAL = re.compile(r'(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.])')
+
+
+def to_f32(method_lines):
+    """FP32 twin of the generated FP64 compute method (same recursion graph):
+    compute_f32 with float intermediates, the float Boys table and float
+    rsqrt; used for the small-bound quartets of the mixed-precision build."""
+    out = []
+    for line in method_lines:
+        t = line.replace('static void compute(', 'static void compute_f32(')
+        t = t.replace('const double* __restrict__ btab', 'const float* __restrict__ btab')
+        t = t.replace('double* __restrict__ out', 'float* __restrict__ out')
+        t = t.replace('const double ', 'const float ').replace('double c_', 'float c_').replace('double F[', 'float F[')
+        t = t.replace('boys_function<', 'boys_function_f<').replace('rsqrt(', 'rsqrtf(')
+        if not t.lstrip().startswith('//'):
+            t = _FLOAT_LITERAL.sub(lambda m: m.group(1) + 'f', t)
+        out.append(t)
+    return out
+
 
 def _num(v):
     if isinstance(v, int):

@@ -142,6 +142,7 @@ struct DeviceGlobals {
     bool ready = false;
     int nsm = 0;
     double* boys = nullptr;
+    float* boys_f = nullptr;
     void* prog = nullptr;
     std::vector<CoopClassDev> coop;
     std::vector<int> coop_prim_flops, coop_post_flops;
@@ -160,6 +161,9 @@ int device_globals(int device, DeviceGlobals** out)
         const auto tab = make_boys_table();
         VLX_CUDA(cudaMalloc(&g.boys, tab.size() * sizeof(double)));
         VLX_CUDA(cudaMemcpy(g.boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+        const std::vector<float> tabf(tab.begin(), tab.end());
+        VLX_CUDA(cudaMalloc(&g.boys_f, tabf.size() * sizeof(float)));
+        VLX_CUDA(cudaMemcpy(g.boys_f, tabf.data(), tabf.size() * sizeof(float), cudaMemcpyHostToDevice));
         // warp-cooperative programs (gen_coop.py): magic, count, 16-int headers,
         // 16-byte op records, LIN weights (float64), then the aux int32 stream
         const char* blob = vlx_coop_blob_start;
@@ -296,13 +300,14 @@ struct ClassTasks {
     int compiled = -1;  // index into kQuartetClasses
     int coop = -1;      // index into DeviceGlobals::coop
     int la = 0, lb = 0, lc = 0, ld = 0;
-    std::vector<WorkItem> items;
-    size_t offset = 0;
-    long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0;
+    std::vector<WorkItem> items;    // FP64 quartets
+    std::vector<WorkItem> items32;  // FP32 quartets (mixed precision, compiled classes only)
+    size_t offset = 0, offset32 = 0;
+    long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0, fp32_quartets = 0;
 };
 
 struct TaskSet {
-    int ith = 0, rank = 0, nodes = 1, seg = 0;
+    int ith = 0, rank = 0, nodes = 1, seg = 0, ith32 = -1;
     std::vector<ClassTasks> classes;
     WorkItem* d_items = nullptr;
     long long quartets = 0, prim_quartets = 0;
@@ -332,6 +337,7 @@ struct vlx_b200_screener {
     int* d_counters = nullptr;
     int ncounters = 0;
     int seg = 256;
+    int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -491,7 +497,7 @@ int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
 int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** out)
 {
     for (auto& t : s->tasksets)
-        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg) {
+        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg && t.ith32 == s->ith32) {
             *out = &t;
             return VLX_B200_OK;
         }
@@ -500,6 +506,7 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
     ts.rank = rank;
     ts.nodes = nodes;
     ts.seg = s->seg;
+    ts.ith32 = s->ith32;
     std::map<int, int> cls_index;  // key -> position in ts.classes
     long long g = 0;
     const size_t nb = s->blocks.size();
@@ -543,12 +550,29 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                 for (int k0 = kbeg; k0 < kend; k0 += seg) {
                     const int k1 = std::min(kend, k0 + seg);
                     if ((g++ % nodes) != rank) continue;
+                    // mixed precision: kets are bin-sorted, so the quartets whose bound
+                    // 10^-(bin_bra + bin_ket) times max|D| is below the FP32 cutoff
+                    // are the tail [k_mid, k1) of the run
+                    int k_mid = k1;
+                    if (s->ith32 >= 0 && ct.compiled >= 0) {
+                        const int b32 = s->ith32 - bx;
+                        const int kb32 = (b32 <= 0) ? 0 : Pk.bin_off[std::min(b32, 16)];
+                        k_mid = std::min(k1, std::max(k0, kb32));
+                    }
                     WorkItem w;
                     w.blocks = (int)bra | ((int)ket << 16);
                     w.bra = x;
-                    w.kbeg = k0;
-                    w.kend = k1;
-                    ct.items.push_back(w);
+                    if (k_mid > k0) {
+                        w.kbeg = k0;
+                        w.kend = k_mid;
+                        ct.items.push_back(w);
+                    }
+                    if (k1 > k_mid) {
+                        w.kbeg = k_mid;
+                        w.kend = k1;
+                        ct.items32.push_back(w);
+                        ct.fp32_quartets += k1 - k_mid;
+                    }
                     const long long evaluated =
                         (long long)Pb.nuse[x] * (Pk.nuse_prefix[k1] - Pk.nuse_prefix[k0]);
                     ts.quartets += k1 - k0;
@@ -563,17 +587,22 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
     for (auto& ct : ts.classes) {
         ct.offset = total;
         total += ct.items.size();
+        ct.offset32 = total;
+        total += ct.items32.size();
     }
     if (total > 0) {
         std::vector<WorkItem> all;
         all.reserve(total);
-        for (auto& ct : ts.classes) all.insert(all.end(), ct.items.begin(), ct.items.end());
+        for (auto& ct : ts.classes) {
+            all.insert(all.end(), ct.items.begin(), ct.items.end());
+            all.insert(all.end(), ct.items32.begin(), ct.items32.end());
+        }
         VLX_CUDA(cudaMalloc(&ts.d_items, total * sizeof(WorkItem)));
         VLX_CUDA(cudaMemcpy(ts.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));
     }
-    if ((int)ts.classes.size() > s->ncounters) {
+    if (2 * (int)ts.classes.size() > s->ncounters) {
         if (s->d_counters) cudaFree(s->d_counters);
-        s->ncounters = std::max<int>(64, (int)ts.classes.size());
+        s->ncounters = std::max<int>(128, 2 * (int)ts.classes.size());
         VLX_CUDA(cudaMalloc(&s->d_counters, s->ncounters * sizeof(int)));
     }
     // keep the cache small: the SCF changes ithreshold only a few times
@@ -615,11 +644,12 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
                     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
 {
     if (ts->classes.empty()) return VLX_B200_OK;
-    VLX_CUDA(cudaMemsetAsync(s->d_counters, 0, ts->classes.size() * sizeof(int), st));
+    VLX_CUDA(cudaMemsetAsync(s->d_counters, 0, 2 * ts->classes.size() * sizeof(int), st));
     FockArgs a;
     std::memset(&a, 0, sizeof(a));
     a.blocks = s->d_blocks;
     a.boys = s->glob->boys;
+    a.boys_f = s->glob->boys_f;
     a.D = dD;
     a.F = dAcc;
     a.eri = eri;
@@ -630,7 +660,7 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     const int warps_per_block = vlx::kWarpsPerBlock;
     for (size_t c = 0; c < ts->classes.size(); c++) {
         ClassTasks& ct = ts->classes[c];
-        if (ct.items.empty()) continue;
+        if (ct.items.empty() && ct.items32.empty()) continue;
         a.items = ts->d_items + ct.offset;
         a.nitems = (int)ct.items.size();
         a.counter = s->d_counters + c;
@@ -639,8 +669,16 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
         if (ct.compiled >= 0) {
             const auto& e = vlx::kQuartetClasses[ct.compiled];
             const int occ = std::max(1, e.occupancy(mode));
-            const int grid = std::max(1, std::min(want, occ * s->glob->nsm));
-            e.launch(mode, a, grid, st);
+            if (!ct.items.empty()) e.launch(mode, a, std::max(1, std::min(want, occ * s->glob->nsm)), st);
+            if (!ct.items32.empty()) {
+                FockArgs a32 = a;
+                a32.items = ts->d_items + ct.offset32;
+                a32.nitems = (int)ct.items32.size();
+                a32.counter = s->d_counters + ts->classes.size() + c;
+                const int want32 = (int)((ct.items32.size() + warps_per_block - 1) / warps_per_block);
+                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * s->glob->nsm)), st);
+                if (launches) (*launches)++;
+            }
         } else {
             const CoopClassDev& cc = s->glob->coop[ct.coop];
             const int wpb = vlx::coop_warps_per_block(cc);
@@ -1043,7 +1081,7 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
     // the work list must already exist: building it would allocate device memory
     TaskSet* ts = nullptr;
     for (auto& t : s->tasksets)
-        if (t.ith == ith && t.rank == 0 && t.nodes == 1 && t.seg == s->seg) ts = &t;
+        if (t.ith == ith && t.rank == 0 && t.nodes == 1 && t.seg == s->seg && t.ith32 < 0) ts = &t;
     if (known && !ts)
         return fail(VLX_B200_ERR_ARGUMENT,
                     "fock_build_noalloc: no work list for ithreshold " + std::to_string(ith) +
@@ -1202,6 +1240,18 @@ int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const
     return rc;
 }
 
+int vlx_b200_set_fp32_threshold(vlx_b200_screener* s, double cutoff, double max_abs_density)
+{
+    if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
+    if (cutoff <= 0.0 || max_abs_density <= 0.0) {
+        s->ith32 = -1;
+        return VLX_B200_OK;
+    }
+    // bound 10^-(bin_bra + bin_ket) * max|D| < cutoff  <=>  bin sum >= floor(log10(max|D| / cutoff)) + 1
+    s->ith32 = std::max(0, (int)std::floor(std::log10(max_abs_density / cutoff)) + 1);
+    return VLX_B200_OK;
+}
+
 int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
 {
     if (!s || !eri_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
@@ -1276,6 +1326,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         p.shell_quartets = ct.quartets;
         p.prim_quartets = ct.prim_quartets;
         p.flops = class_flops(s, ct);
+        p.fp32_quartets = ct.fp32_quartets;
     }
     for (auto& x : ev) {
         cudaEventDestroy(x.first);

@@ -217,15 +217,23 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
             const int jj = act ? j : (w.kend - 1);
             const PairView ket = make_view(kb, jj);
             double f[C::NSPH];
-            C::compute(bra, ket, a.boys, f);
+            if (mode & MODE_F32) {
+                float g[C::NSPH];
+                C::compute_f32(bra, ket, a.boys_f, g);
+#pragma unroll
+                for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
+            } else {
+                C::compute(bra, ket, a.boys, f);
+            }
             const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
-            if (mode == MODE_ERI) {
+            const int dmode = mode & 3;
+            if (dmode == MODE_ERI) {
                 if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, a.nao);
             } else {
                 double s = act ? s_bra : 0.0;
                 if (r0 == s0) s *= 0.5;
                 if (bbi == kbi && jj == w.bra) s *= 0.5;
-                if (mode == MODE_FOCK_SYM)
+                if (dmode == MODE_FOCK_SYM)
                     digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);
                 else
                     digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);

@@ -44,6 +44,9 @@ struct WorkItem {
 };
 
 enum KernelMode { MODE_FOCK_SYM = 0, MODE_FOCK_GEN = 1, MODE_ERI = 2 };
+// or-ed into the mode of a compiled-class launch: evaluate the quartets with
+// the FP32 recursion (digestion and accumulation stay FP64)
+constexpr int MODE_F32 = 4;
 
 struct FockArgs {
     const PairBlockDev* blocks;
@@ -51,6 +54,7 @@ struct FockArgs {
     int nitems;
     int* counter;             // work-queue head for this launch (zeroed before)
     const double* boys;       // Chebyshev table
+    const float* boys_f;      // the same table rounded to float (mixed precision)
     const double* D;          // density, nao x nao row-major
     double* F;                // accumulator, nao x nao row-major
     double* eri;              // MODE_ERI: nao^4 tensor

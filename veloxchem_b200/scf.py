@@ -110,6 +110,11 @@ class ScfRestrictedDriver:
         self.eri_thresh = 1.0e-12
         self.ovl_thresh = 1.0e-6
         self.guess = 'sad'
+        # mixed precision: quartets with Schwarz bound x max|D| < fp32_cutoff in
+        # FP32 while the electronic gradient is above fp32_until_grad; the
+        # final iterations are FP64, so the converged energy is the FP64 one
+        self.fp32_cutoff = 0.0
+        self.fp32_until_grad = 1.0e-4
         self.history = []
         self.timings = {}
 
@@ -167,6 +172,11 @@ class ScfRestrictedDriver:
         for it in range(1, self.max_iter + 1):
             ith = int(-math.log10(self.dyn_threshold(e_grad)))
             D = 0.5 * (D + D.T).contiguous()
+            mixed = self.fp32_cutoff > 0.0 and e_grad > self.fp32_until_grad
+            if mixed:
+                screener.set_fp32_threshold(self.fp32_cutoff, float(torch.max(torch.abs(D))))
+            else:
+                screener.set_fp32_threshold(0.0, 0.0)
             t0 = time.perf_counter()
             nat.check(nat.lib().vlx_b200_fock_build_device(screener.handle, ctypes.c_void_p(D.data_ptr()), 1, b'2jk',
                                                             1.0, 0.0, ith, ctypes.c_void_p(F2e.data_ptr()),
@@ -181,7 +191,7 @@ class ScfRestrictedDriver:
             err = X.T @ (fds - fds.T) @ X
             e_grad = 2.0 * float(torch.linalg.norm(err))
             self.history.append({'iteration': it, 'energy': energy, 'delta_e': energy - e_old, 'e_grad': e_grad,
-                                 'ithreshold': ith, 'time_s': time.perf_counter() - t_start})
+                                 'ithreshold': ith, 'mixed': mixed, 'time_s': time.perf_counter() - t_start})
             e_old = energy
             if e_grad < self.conv_thresh:
                 converged = True
@@ -195,6 +205,7 @@ class ScfRestrictedDriver:
             e, c = torch.linalg.eigh(X.T @ F_eff @ X)
             C = X @ c[:, :nocc]
             D = C @ C.T
+        screener.set_fp32_threshold(0.0, 0.0)
         self.timings['fock_ms_total'] = fock_ms
         self.timings['total_s'] = time.perf_counter() - t_start
         e, c = torch.linalg.eigh(X.T @ F @ X)

@@ -107,6 +107,12 @@ class T4CScreener:
         nat.check(nat.lib().vlx_b200_screener_pair_info(self.handle, nat.iptr(info), nat.dptr(maxv)), 'pair_info')
         return info, maxv
 
+    def set_fp32_threshold(self, cutoff, max_abs_density):
+        """Mixed precision: quartets with Schwarz bound x max|D| below cutoff in
+        FP32 for the following builds (cutoff <= 0: FP64 only)."""
+        nat.check(nat.lib().vlx_b200_set_fp32_threshold(self.handle, float(cutoff), float(max_abs_density)),
+                  'set_fp32_threshold')
+
     def set_block_size_factor(self, factor):
         nat.check(nat.lib().vlx_b200_set_block_size_factor(self.handle, int(factor)), 'set_block_size_factor')
 
