@@ -27,6 +27,7 @@ extern "C" {
 #define VLX_B200_ERR_NO_DEVICE 4   /* no CUDA device available */
 
 typedef struct vlx_b200_screener vlx_b200_screener;
+typedef struct vlx_b200_batch vlx_b200_batch;
 
 /* Statistics of one build (any field may be ignored by passing NULL). */
 typedef struct {
@@ -85,9 +86,12 @@ int vlx_b200_set_block_size_factor(vlx_b200_screener* screener, int factor);
 
 /* One Fock matrix.  density / fock_out: host nao x nao.  symmetric != 0 for a
  * symmetric density (reference mat_t::symmetric), else general.
- * label: "2jk", "2jkx", "j", "k", "kx" ("j_rs", "k_rs", "kx_rs" alias the
- * last three); an unknown label yields a zero matrix, as in the reference.
- * omega must be 0 (range-separated integrals are not compiled in).
+ * label: "2jk", "2jkx", "j", "k", "kx", and "j_rs", "k_rs", "kx_rs", which
+ * weight as the last three but use the erf-attenuated operator erf(omega r)/r
+ * (reference T4CMatrixDistributor::need_omega, Boys rescaling in
+ * CBoysFunc::compute with omega, src/math/BoysFunc.hpp:24892-24999); omega is
+ * ignored for the other labels and must be finite and >= 0.  An unknown
+ * label yields a zero matrix, as in the reference.
  * Quartets with bin(bra) + bin(ket) <= ithreshold are included.
  * Replaces CFockDriver::compute(screener, density, label, exchange_factor,
  * omega, ithreshold) (src/t4c_func/FockDriver.cpp:120-172). */
@@ -198,7 +202,7 @@ typedef struct {
 } vlx_b200_class_profile;
 
 /* A device-resident build (as vlx_b200_fock_build_device, ithreshold and
- * label as there, omega = 0) with one CUDA-event pair around each quartet-class
+ * label as there, but not the range-separated labels) with one CUDA-event pair around each quartet-class
  * launch on `stream`; synchronises and fills up to max_classes records.
  * Measurement entry point, no counterpart in the reference. */
 int vlx_b200_fock_profile(vlx_b200_screener* screener, const double* d_density, int symmetric, const char* label,
@@ -209,6 +213,64 @@ int vlx_b200_fock_profile(vlx_b200_screener* screener, const double* d_density, 
  * FMA-chain probe kernel): the roofline denominator of the FP64 recursions.
  * Measurement entry point, no counterpart in the reference. */
 int vlx_b200_fp64_peak(int device, double* tflops);
+
+/* ---- batched many-molecule builds (no counterpart in the reference, whose
+ * FockDriver builds one molecule per call: CFockDriver::compute,
+ * src/t4c_func/FockDriver.cpp:120-172, is what each molecule's result equals).
+ *
+ * A batch groups screeners of independent molecules on one device; a build
+ * runs every quartet class of every molecule as one persistent launch per
+ * class, captured (use_graph != 0) into a CUDA graph that is replayed while
+ * the pointers, label, exchange factor, omega and ithreshold stay the same.
+ * The screeners must outlive the batch and must not be repartitioned. */
+int vlx_b200_batch_create(vlx_b200_batch** batch, vlx_b200_screener* const* screeners, int nmolecules);
+int vlx_b200_batch_destroy(vlx_b200_batch* batch);
+
+/* nmolecules + 1 element offsets of the packed matrices: molecule k's
+ * nao_k x nao_k row-major block starts at offsets[k]; offsets[n] is the total. */
+int vlx_b200_batch_offsets(const vlx_b200_batch* batch, long long* offsets);
+
+/* One Fock build per molecule from device-resident packed densities into
+ * device-resident packed Fock matrices (symmetric, label, exchange_factor,
+ * omega, ithreshold as in vlx_b200_fock_build, shared by all molecules).
+ * Enqueued on `stream` (NULL: the batch's own stream); returns without
+ * synchronising.  A change of d_densities synchronises the device once (the
+ * per-molecule records are rewritten). */
+int vlx_b200_batch_fock_build(vlx_b200_batch* batch, const double* d_densities, int symmetric, const char* label,
+                              double exchange_factor, double omega, int ithreshold, double* d_focks, void* stream,
+                              int use_graph, vlx_b200_stats* stats);
+
+/* ---- learned initial guess: kernels of the density-block network (no
+ * counterpart in the reference, whose guesses are SAD, core and restart).
+ * All pointers are device memory; row-major; launches are enqueued on
+ * `stream` and return without synchronising. */
+
+/* Y[M, N] = act(X[M, K] W[N, K]^T + b[N]); act = SiLU if silu != 0, else
+ * identity; Z (NULL allowed) receives the pre-activation for training. */
+int vlx_b200_mlp_linear(const float* X, const float* W, const float* b, float* Z, float* Y, int M, int K, int N,
+                        int silu, void* stream);
+
+/* Inference form: W in BF16 (as written by vlx_b200_to_bf16), X rounded to
+ * BF16 on load, FP32 accumulation and output. */
+int vlx_b200_mlp_linear_bf16(const float* X, const void* W_bf16, const float* b, float* Y, int M, int K, int N,
+                             int silu, void* stream);
+
+/* Backward of vlx_b200_mlp_linear: from dY[M, N] (and Z when silu != 0, with
+ * dZ[M, N] as scratch) writes dW[N, K], db[N] and, when dX != NULL, dX[M, K]. */
+int vlx_b200_mlp_linear_backward(const float* X, const float* W, const float* Z, const float* dY, float* dZ,
+                                 float* dX, float* dW, float* db, int M, int K, int N, int silu, void* stream);
+
+/* Masked squared error: dY = 2 mask (Y - T) / count; *d_loss_sum (device,
+ * FP64) += sum mask (Y - T)^2. */
+int vlx_b200_mlp_mse(const float* Y, const float* T, const float* mask, float* dY, double* d_loss_sum, long long n,
+                     double count, void* stream);
+
+/* One Adam step (bias-corrected moments) at step >= 1. */
+int vlx_b200_adam_step(float* params, const float* grads, float* m, float* v, long long n, float lr, float beta1,
+                       float beta2, float eps, int step, void* stream);
+
+/* FP32 -> BF16 (round to nearest even). */
+int vlx_b200_to_bf16(const float* x, void* y_bf16, long long n, void* stream);
 
 #ifdef __cplusplus
 }

@@ -171,15 +171,40 @@ def test_block_size_factor_does_not_change_result():
     assert np.max(np.abs(a - b)) < 1e-12
 
 
-def test_omega_is_rejected_loudly():
-    from veloxchem_b200._native import NativeError
-    g, mol, bas = load_golden('h2o_sto3g.npz')
+@pytest.mark.parametrize('label,xfac', [('k_rs', 0.0), ('kx_rs', 0.21)])
+def test_range_separated_exchange_against_golden(label, xfac):
+    """erf-attenuated K (omega = 0.63) against the reference's golden matrix
+    (its tests/test_fock_erf_driver.py: k_rs with xfac 0, kx_rs with 0.21)."""
+    g, mol, bas = load_golden('h2o_dimer_tzvp.npz')
     s = _screener(mol, bas)
     from veloxchem_b200 import FockDriver, make_matrix, mat_t
     m = make_matrix(bas, mat_t.symmetric)
     m.set_values(g['density'])
+    f = FockDriver()._compute_fock_omp(s, m, label, xfac, 0.63, 15).full_matrix().to_numpy()
+    scale = 1.0 if label == 'k_rs' else xfac
+    assert np.max(np.abs(f - scale * g['erf_k'])) < TOL
+
+
+def test_range_separated_j_against_oracle_and_limits():
+    """j_rs against the compiled reference; omega is ignored by plain labels,
+    omega = 0 gives a zero matrix, a negative omega is an error."""
+    from oracle.oracle import RefOracle
+    from veloxchem_b200._native import NativeError
+    g, mol, bas = load_golden('h2o_dimer_svpd.npz')
+    s = _screener(mol, bas)
+    from veloxchem_b200 import FockDriver, make_matrix, mat_t
+    m = make_matrix(bas, mat_t.symmetric)
+    m.set_values(g['density'])
+    drv = FockDriver()
+    j_rs = drv._compute_fock_omp(s, m, 'j_rs', 0.0, 0.4, 15).full_matrix().to_numpy()
+    ref = RefOracle(mol, bas).fock(g['density'], 'j_rs', 0.0, 0.4, 15)
+    assert np.max(np.abs(j_rs - ref)) < TOL
+    assert np.max(np.abs(j_rs - g['j'])) > 1e-3
+    j = drv._compute_fock_omp(s, m, 'j', 0.0, 0.4, 15).full_matrix().to_numpy()
+    assert np.max(np.abs(j - g['j'])) < TOL
+    assert np.all(drv._compute_fock_omp(s, m, 'k_rs', 0.0, 0.0, 15).full_matrix().to_numpy() == 0.0)
     with pytest.raises(NativeError):
-        FockDriver().compute(s, m, 'kx_rs', 1.0, 0.3, 15)
+        drv._compute_fock_omp(s, m, 'k_rs', 0.0, -0.3, 15)
 
 
 def test_large_cluster_properties():

@@ -76,3 +76,12 @@ def test_cluster_fixture_from_reference():
     assert o.nao == 96
     assert np.max(np.abs(o.fock(g['density'], 'j', 1.0, 12) - g['j'])) < 1e-12
     assert np.max(np.abs(o.fock(g['density'], 'k', 1.0, 12) - g['k'])) < 1e-12
+
+
+@pytest.mark.skipif(not ref_available(), reason='reference oracle not built (make -C oracle reference)')
+def test_compiled_reference_erf_exchange_golden():
+    """The compiled reference reproduces its own erf-attenuated K golden
+    (omega 0.63), so it can check the range-separated labels."""
+    g, mol, bas = load_golden('h2o_dimer_tzvp.npz')
+    ref = RefOracle(mol, bas)
+    assert np.max(np.abs(ref.fock(g['density'], 'k_rs', 0.0, 0.63, 15) - g['erf_k'])) < 1e-12

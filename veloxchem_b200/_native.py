@@ -49,6 +49,21 @@ SIGNATURES = {
     'vlx_b200_set_fp32_threshold': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     'vlx_b200_fock_build_noalloc': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    'vlx_b200_mlp_linear': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _vp]),
+    'vlx_b200_mlp_linear_bf16': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, _vp]),
+    'vlx_b200_mlp_linear_backward': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    'vlx_b200_mlp_mse': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_double, _vp]),
+    'vlx_b200_adam_step': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_float, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_float, ctypes.c_int, _vp]),
+    'vlx_b200_to_bf16': (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
+    'vlx_b200_batch_create': (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int]),
+    'vlx_b200_batch_destroy': (ctypes.c_int, [_vp]),
+    'vlx_b200_batch_offsets': (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    'vlx_b200_batch_fock_build': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]),
 }
 
 

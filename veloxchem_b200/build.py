@@ -75,7 +75,8 @@ def build(jobs=None, lmax=3, verbose=True):
     if not asm.exists() or asm.read_text() != asm_text:
         asm.write_text(asm_text)
     hdr = _headers_digest()
-    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_onee.cu', CSRC / 'vlx_host.cu']
+    sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_onee.cu', CSRC / 'vlx_mlp.cu',
+                                                CSRC / 'vlx_host.cu']
     objs = [OBJ / (s.stem + '.o') for s in sources]
     jobs = jobs or os.cpu_count() or 4
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:

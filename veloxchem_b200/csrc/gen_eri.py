@@ -206,7 +206,7 @@ class ClassGen:
         method_start = len(lines)
         w('    template <class BraT, class KetT>')
         w('    __device__ __forceinline__ static void compute(const BraT& bra, const KetT& ket, const double* __restrict__ btab,')
-        w('                                                   double* __restrict__ out)')
+        w('                                                   const double om2, double* __restrict__ out)')
         w('    {')
         for ie in range(len(e_t)):
             for jf in range(len(f_t)):
@@ -231,10 +231,16 @@ class ClassGen:
         w('                const double WQx = rh * PQx, WQy = rh * PQy, WQz = rh * PQz;')
         w('                const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);')
         w('                double F[%d];' % (L + 1))
-        w('                boys_function<%d>(T, F, btab);' % L)
-        w('                const double pref = kab * kcd * r;')
+        # erf-attenuated operator: F_m(T) -> s^(2m+1) F_m(s^2 T), s^2 = om2 / (om2 + rho)
+        w('                const double s2 = (om2 > 0.0) ? om2 / (om2 + rho) : 1.0;')
+        w('                boys_function<%d>(T * s2, F, btab);' % L)
+        w('                double pref = kab * kcd * r;')
+        w('                if (om2 > 0.0) pref *= sqrt(s2);')
         w('                #pragma unroll')
-        w('                for (int m = 0; m <= %d; m++) F[m] *= pref;' % L)
+        w('                for (int m = 0; m <= %d; m++) {' % L)
+        w('                    F[m] *= pref;')
+        w('                    if (om2 > 0.0) pref *= s2;')
+        w('                }')
         w('                (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;')
         w('                (void)QDx; (void)QDy; (void)QDz; (void)PBx; (void)PBy; (void)PBz;')
         w('                (void)hiz; (void)hie; (void)hizh; (void)rz; (void)rh;')
@@ -509,6 +515,7 @@ def to_f32(method_lines):
         t = t.replace('double* __restrict__ out', 'float* __restrict__ out')
         t = t.replace('const double ', 'const float ').replace('double c_', 'float c_').replace('double F[', 'float F[')
         t = t.replace('boys_function<', 'boys_function_f<').replace('rsqrt(', 'rsqrtf(')
+        t = re.sub(r'(?<![r\w])sqrt\(', 'sqrtf(', t).replace('double pref', 'float pref')
         if not t.lstrip().startswith('//'):
             t = _FLOAT_LITERAL.sub(lambda m: m.group(1) + 'f', t)
         out.append(t)

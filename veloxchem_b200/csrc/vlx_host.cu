@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -629,6 +630,17 @@ bool label_weights(const char* label, int symmetric, double xfac, double* cj, do
     return false;
 }
 
+// Labels j_rs, k_rs, kx_rs use the erf(omega r)/r operator (reference
+// T4CMatrixDistributor::need_omega, T4CMatrixDistributor.cpp:51-54); omega is
+// ignored for the other labels.  With omega = 0 the attenuated integrals, and
+// so the matrix, vanish (the reference's Boys rescaling by omega / sqrt(omega^2
+// + rho), BoysFunc.hpp:24930-24980): the label then contributes nothing.
+bool label_is_range_separated(const char* label)
+{
+    const std::string l(label ? label : "");
+    return l == "j_rs" || l == "k_rs" || l == "kx_rs";
+}
+
 int ensure_buffers(vlx_b200_screener* s)
 {
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
@@ -638,59 +650,88 @@ int ensure_buffers(vlx_b200_screener* s)
     return VLX_B200_OK;
 }
 
-// Enqueues all class kernels of a task set on `st`; F (accumulator) must be zeroed.
-int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
-                    double cj, double ck, cudaStream_t st, long long* launches,
-                    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
+// Where the class kernels of one build read and write: the pair-block table,
+// the work-queue heads (two per class: FP64 and FP32 items) and the molecule
+// data (one molecule, or per-molecule records of a batched build).
+struct LaunchCtx {
+    const PairBlockDev* blocks = nullptr;
+    DeviceGlobals* glob = nullptr;
+    int* counters = nullptr;
+    vlx::MolDev mol{};
+    const vlx::MolDev* mols = nullptr;
+};
+
+// Enqueues all class kernels of a task set on `st`; the accumulators must be zeroed.
+int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double cj, double ck, double omega2,
+                cudaStream_t st, long long* launches,
+                std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
 {
     if (ts->classes.empty()) return VLX_B200_OK;
-    VLX_CUDA(cudaMemsetAsync(s->d_counters, 0, 2 * ts->classes.size() * sizeof(int), st));
+    VLX_CUDA(cudaMemsetAsync(L.counters, 0, 2 * ts->classes.size() * sizeof(int), st));
     FockArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.blocks = s->d_blocks;
-    a.boys = s->glob->boys;
-    a.boys_f = s->glob->boys_f;
-    a.D = dD;
-    a.F = dAcc;
+    a.blocks = L.blocks;
+    a.boys = L.glob->boys;
+    a.boys_f = L.glob->boys_f;
+    a.mol = L.mol;
+    a.mols = L.mols;
     a.eri = eri;
-    a.nao = s->nao;
-    for (int l = 0; l <= VLX_LMAX; l++) a.nl[l] = s->nl[l];
     a.cj = cj;
     a.ck = ck;
+    a.omega2 = omega2;
     const int warps_per_block = vlx::kWarpsPerBlock;
+    const int nsm = L.glob->nsm;
     for (size_t c = 0; c < ts->classes.size(); c++) {
         ClassTasks& ct = ts->classes[c];
         if (ct.items.empty() && ct.items32.empty()) continue;
         a.items = ts->d_items + ct.offset;
         a.nitems = (int)ct.items.size();
-        a.counter = s->d_counters + c;
+        a.counter = L.counters + c;
         const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].first, st));
         if (ct.compiled >= 0) {
             const auto& e = vlx::kQuartetClasses[ct.compiled];
             const int occ = std::max(1, e.occupancy(mode));
-            if (!ct.items.empty()) e.launch(mode, a, std::max(1, std::min(want, occ * s->glob->nsm)), st);
+            if (!ct.items.empty()) {
+                e.launch(mode, a, std::max(1, std::min(want, occ * nsm)), st);
+                if (launches) (*launches)++;
+            }
             if (!ct.items32.empty()) {
                 FockArgs a32 = a;
                 a32.items = ts->d_items + ct.offset32;
                 a32.nitems = (int)ct.items32.size();
-                a32.counter = s->d_counters + ts->classes.size() + c;
+                a32.counter = L.counters + ts->classes.size() + c;
                 const int want32 = (int)((ct.items32.size() + warps_per_block - 1) / warps_per_block);
-                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * s->glob->nsm)), st);
+                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * nsm)), st);
                 if (launches) (*launches)++;
             }
         } else {
-            const CoopClassDev& cc = s->glob->coop[ct.coop];
+            const CoopClassDev& cc = L.glob->coop[ct.coop];
             const int wpb = vlx::coop_warps_per_block(cc);
-            const int cap = vlx::coop_blocks_per_sm(cc) * s->glob->nsm;
+            const int cap = vlx::coop_blocks_per_sm(cc) * nsm;
             const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
             vlx::launch_coop_quartet(mode, a, cc, grid, st);
+            if (launches) (*launches)++;
         }
         VLX_CUDA(cudaGetLastError());
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].second, st));
-        if (launches) (*launches)++;
     }
     return VLX_B200_OK;
+}
+
+int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
+                    double cj, double ck, double omega2, cudaStream_t st, long long* launches,
+                    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
+{
+    LaunchCtx L;
+    L.blocks = s->d_blocks;
+    L.glob = s->glob;
+    L.counters = s->d_counters;
+    L.mol.D = dD;
+    L.mol.F = dAcc;
+    L.mol.nao = s->nao;
+    for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
+    return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, st, launches, events);
 }
 
 // Algorithmic FP64 flops of one class launch: per primitive quartet the
@@ -715,10 +756,12 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
                  double xfac, double omega, int ith, double* dF, cudaStream_t st, long long* quartets,
                  long long* prim, long long* launches)
 {
-    if (omega != 0.0) return fail(VLX_B200_ERR_UNSUPPORTED, "range-separated (omega != 0) integrals not compiled in");
     if (nodes < 1 || rank < 0 || rank >= nodes) return fail(VLX_B200_ERR_ARGUMENT, "invalid rank / nodes");
+    if (!std::isfinite(omega) || omega < 0.0) return fail(VLX_B200_ERR_ARGUMENT, "omega must be finite and >= 0");
     double cj = 0.0, ck = 0.0;
-    const bool known = label_weights(label, symmetric, xfac, &cj, &ck);
+    const bool rs = label_is_range_separated(label);
+    const bool known = label_weights(label, symmetric, xfac, &cj, &ck) && !(rs && omega == 0.0);
+    const double omega2 = rs ? omega * omega : 0.0;
     int rc = ensure_buffers(s);
     if (rc) return rc;
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
@@ -728,7 +771,7 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
         rc = build_tasks(s, ith, rank, nodes, &ts);
         if (rc) return rc;
         rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dD, s->d_acc, nullptr, cj,
-                             ck, st, launches);
+                             ck, omega2, st, launches);
         if (rc) return rc;
         if (quartets) *quartets += ts->quartets;
         if (prim) *prim += ts->prim_quartets;
@@ -782,6 +825,9 @@ extern "C" {
 const char* vlx_b200_version(void) { return "vlx_b200 0.1 (sm_100a, FP64 HGP, L<=3)"; }
 
 const char* vlx_b200_last_error(void) { return g_err.c_str(); }
+
+// Error hook of the other translation units of the library (not in the public header).
+int vlx_b200_set_error_internal(int code, const char* msg) { return fail(code, msg ? msg : ""); }
 
 int vlx_b200_device_count(int* count)
 {
@@ -1075,9 +1121,10 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
         return fail(VLX_B200_ERR_ARGUMENT, "fock_build_noalloc: " + std::to_string(s->nao) +
                                                " basis functions exceed the static scratch limit of " +
                                                std::to_string(VLX_B200_NOALLOC_MAX_NAO));
-    if (omega != 0.0) return fail(VLX_B200_ERR_UNSUPPORTED, "range-separated (omega != 0) integrals not compiled in");
+    if (!std::isfinite(omega) || omega < 0.0) return fail(VLX_B200_ERR_ARGUMENT, "omega must be finite and >= 0");
     double cj = 0.0, ck = 0.0;
-    const bool known = label_weights(label, symmetric, xfac, &cj, &ck);
+    const bool rs = label_is_range_separated(label);
+    const bool known = label_weights(label, symmetric, xfac, &cj, &ck) && !(rs && omega == 0.0);
     // the work list must already exist: building it would allocate device memory
     TaskSet* ts = nullptr;
     for (auto& t : s->tasksets)
@@ -1102,12 +1149,13 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
         std::memset(&a, 0, sizeof(a));
         a.blocks = s->d_blocks;
         a.boys = s->glob->boys;
-        a.D = d_density;
-        a.F = sc.acc;
-        a.nao = s->nao;
-        for (int l = 0; l <= VLX_LMAX; l++) a.nl[l] = s->nl[l];
+        a.mol.D = d_density;
+        a.mol.F = sc.acc;
+        a.mol.nao = s->nao;
+        for (int l = 0; l <= VLX_LMAX; l++) a.mol.nl[l] = s->nl[l];
         a.cj = cj;
         a.ck = ck;
+        a.omega2 = rs ? omega * omega : 0.0;
         const int mode = symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN;
         for (size_t c = 0; c < ts->classes.size(); c++) {
             const ClassTasks& ct = ts->classes[c];
@@ -1266,7 +1314,7 @@ int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
     if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     if (!rc) rc = ensure_buffers(s);
     if (!rc) rc = build_tasks(s, ith, 0, 1, &ts);
-    if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, s->stream, nullptr);
+    if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, 0.0, s->stream, nullptr);
     if (!rc) {
         e = cudaMemcpyAsync(eri_out, d_eri, bytes, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -1286,6 +1334,8 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
     double cj = 0.0, ck = 0.0;
     if (!label_weights(label, symmetric, xfac, &cj, &ck)) return fail(VLX_B200_ERR_ARGUMENT, "unknown label");
+    if (label_is_range_separated(label))
+        return fail(VLX_B200_ERR_ARGUMENT, "fock_profile: range-separated labels need omega; use vlx_b200_fock_build");
     int rc = ensure_buffers(s);
     if (rc) return rc;
     TaskSet* ts = nullptr;
@@ -1300,7 +1350,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
     rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, st, nullptr, &ev);
+                         cj, ck, 0.0, st, nullptr, &ev);
     if (!rc && symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
         symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
@@ -1386,6 +1436,332 @@ int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F)
     cudaFree(dT);
     cudaFree(dF);
     if (e != cudaSuccess) return fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    return VLX_B200_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batched builds
+//
+// Fock builds of many independent molecules as one set of launches: the pair
+// blocks of all molecules form one block table (each block records its
+// molecule), the work items of one quartet class from every molecule form one
+// queue, and each class is one persistent launch over all molecules; the
+// kernels take D, F and the basis dimensions of the block's molecule from a
+// per-molecule record.  Densities and Fock matrices are packed: molecule k's
+// nao_k x nao_k block starts at element offset off[k].  The launch sequence
+// (accumulator clear, queue-head clear, class launches, symmetrisation) is
+// captured once into a CUDA graph per (pointers, label, threshold) and
+// replayed.  No counterpart in the reference, whose FockDriver builds one
+// molecule per call.
+
+__global__ void symmetrize_batch_kernel(const double* __restrict__ acc, double* __restrict__ out,
+                                        const long long* __restrict__ off, const int* __restrict__ nao)
+{
+    __shared__ double tile[32][33];
+    const int mol = blockIdx.z;
+    const int n = nao[mol];
+    const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x;
+    if (bx * 32 >= n || by * 32 >= n) return;  // whole block: no barrier is skipped by part of it
+    acc += off[mol];
+    out += off[mol];
+    for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+        const int r = bx * 32 + ty, c = by * 32 + tx;
+        tile[ty][tx] = (r < n && c < n) ? acc[(size_t)r * n + c] : 0.0;
+    }
+    __syncthreads();
+    for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+        const int i = by * 32 + ty, j = bx * 32 + tx;
+        if (i < n && j < n) out[(size_t)i * n + j] = acc[(size_t)i * n + j] + tile[tx][ty];
+    }
+}
+
+struct vlx_b200_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;  // capture stream
+    DeviceGlobals* glob = nullptr;
+    std::vector<vlx_b200_screener*> mols;
+    std::vector<long long> off;     // n + 1 element offsets of the packed matrices
+    int max_nao = 0;
+    PairBlockDev* d_blocks = nullptr;
+    vlx::MolDev* d_mols = nullptr;
+    long long* d_off = nullptr;
+    int* d_nao = nullptr;
+    double* d_acc = nullptr;
+    int* d_counters = nullptr;
+    int ncounters = 0;
+    std::vector<TaskSet> merged;    // one per ithreshold
+    // graph of the last (D, F, symmetric, weights, omega, ithreshold)
+    cudaGraphExec_t exec = nullptr;
+    const double* key_D = nullptr;
+    double* key_F = nullptr;
+    int key_sym = -1, key_ith = -1;
+    double key_cj = 0.0, key_ck = 0.0, key_om2 = -1.0;
+    const double* mols_D = nullptr;  // D of the uploaded per-molecule records
+    long long launches = 0;          // kernel launches of one build
+};
+
+namespace {
+
+int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
+{
+    for (auto& t : b->merged)
+        if (t.ith == ith) {
+            *out = &t;
+            return VLX_B200_OK;
+        }
+    TaskSet m;
+    m.ith = ith;
+    std::map<std::array<int, 4>, int> cls;
+    int boff = 0;
+    for (size_t k = 0; k < b->mols.size(); k++) {
+        vlx_b200_screener* s = b->mols[k];
+        TaskSet* t = nullptr;
+        int rc = build_tasks(s, ith, 0, 1, &t);
+        if (rc) return rc;
+        for (const ClassTasks& ct : t->classes) {
+            const std::array<int, 4> key{ct.la, ct.lb, ct.lc, ct.ld};
+            auto it = cls.find(key);
+            if (it == cls.end()) {
+                ClassTasks n;
+                n.compiled = ct.compiled;
+                n.coop = ct.coop;
+                n.la = ct.la;
+                n.lb = ct.lb;
+                n.lc = ct.lc;
+                n.ld = ct.ld;
+                it = cls.emplace(key, (int)m.classes.size()).first;
+                m.classes.push_back(std::move(n));
+            }
+            ClassTasks& d = m.classes[it->second];
+            for (int f = 0; f < 2; f++) {
+                const std::vector<WorkItem>& src = f ? ct.items32 : ct.items;
+                std::vector<WorkItem>& dst = f ? d.items32 : d.items;
+                for (WorkItem w : src) {
+                    const int bb = (w.blocks & 0xffff) + boff, kb = (w.blocks >> 16) + boff;
+                    w.blocks = bb | (kb << 16);
+                    dst.push_back(w);
+                }
+            }
+            d.quartets += ct.quartets;
+            d.prim_quartets += ct.prim_quartets;
+            d.ref_prim_quartets += ct.ref_prim_quartets;
+            d.fp32_quartets += ct.fp32_quartets;
+        }
+        m.quartets += t->quartets;
+        m.prim_quartets += t->prim_quartets;
+        boff += (int)s->h_blocks.size();
+    }
+    size_t total = 0;
+    for (auto& ct : m.classes) {
+        ct.offset = total;
+        total += ct.items.size();
+        ct.offset32 = total;
+        total += ct.items32.size();
+    }
+    if (total > 0) {
+        std::vector<WorkItem> all;
+        all.reserve(total);
+        for (auto& ct : m.classes) {
+            all.insert(all.end(), ct.items.begin(), ct.items.end());
+            all.insert(all.end(), ct.items32.begin(), ct.items32.end());
+        }
+        VLX_CUDA(cudaMalloc(&m.d_items, total * sizeof(WorkItem)));
+        VLX_CUDA(cudaMemcpy(m.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    }
+    if (2 * (int)m.classes.size() > b->ncounters) {
+        if (b->d_counters) cudaFree(b->d_counters);
+        b->ncounters = std::max<int>(128, 2 * (int)m.classes.size());
+        VLX_CUDA(cudaMalloc(&b->d_counters, b->ncounters * sizeof(int)));
+    }
+    b->merged.push_back(std::move(m));
+    *out = &b->merged.back();
+    return VLX_B200_OK;
+}
+
+// The launch sequence of one batched build on `st`.
+int batch_enqueue(vlx_b200_batch* b, TaskSet* ts, bool known, int symmetric, double cj, double ck, double omega2,
+                  double* d_focks, cudaStream_t st, long long* launches)
+{
+    const long long total = b->off.back();
+    VLX_CUDA(cudaMemsetAsync(b->d_acc, 0, (size_t)std::max<long long>(total, 1) * sizeof(double), st));
+    if (known) {
+        LaunchCtx L;
+        L.blocks = b->d_blocks;
+        L.glob = b->glob;
+        L.counters = b->d_counters;
+        L.mols = b->d_mols;
+        const int rc = enqueue_ctx(L, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, nullptr, cj, ck,
+                                   omega2, st, launches);
+        if (rc) return rc;
+    }
+    if (symmetric) {
+        const int t = (b->max_nao + 31) / 32;
+        const dim3 grid(t, t, (unsigned)b->mols.size()), blk(32, 8);
+        symmetrize_batch_kernel<<<grid, blk, 0, st>>>(b->d_acc, d_focks, b->d_off, b->d_nao);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    } else {
+        VLX_CUDA(cudaMemcpyAsync(d_focks, b->d_acc, (size_t)total * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    return VLX_B200_OK;
+}
+
+void batch_release_graph(vlx_b200_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->key_D = nullptr;
+    b->key_F = nullptr;
+    b->key_sym = -1;
+    b->key_ith = -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screeners, int n)
+{
+    if (!out || !screeners || n < 1 || n > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: bad arguments");
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        if (!screeners[k]) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: null screener");
+        if (screeners[k]->device != screeners[0]->device)
+            return fail(VLX_B200_ERR_ARGUMENT, "batch_create: screeners on different devices");
+    }
+    std::unique_ptr<vlx_b200_batch> b(new vlx_b200_batch());
+    b->device = screeners[0]->device;
+    b->glob = screeners[0]->glob;
+    b->mols.assign(screeners, screeners + n);
+    b->off.assign(n + 1, 0);
+    std::vector<PairBlockDev> blocks;
+    std::vector<int> nao(n);
+    for (int k = 0; k < n; k++) {
+        const vlx_b200_screener* s = screeners[k];
+        nao[k] = s->nao;
+        b->max_nao = std::max(b->max_nao, s->nao);
+        b->off[k + 1] = b->off[k] + (long long)s->nao * s->nao;
+        for (PairBlockDev d : s->h_blocks) {
+            d.mol = k;
+            blocks.push_back(d);
+        }
+    }
+    if (blocks.size() > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: more than 65535 pair blocks");
+    VLX_CUDA(cudaSetDevice(b->device));
+    VLX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    VLX_CUDA(cudaMalloc(&b->d_blocks, std::max<size_t>(1, blocks.size()) * sizeof(PairBlockDev)));
+    if (!blocks.empty())
+        VLX_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), blocks.size() * sizeof(PairBlockDev), cudaMemcpyHostToDevice));
+    VLX_CUDA(cudaMalloc(&b->d_mols, n * sizeof(vlx::MolDev)));
+    VLX_CUDA(cudaMalloc(&b->d_off, (n + 1) * sizeof(long long)));
+    VLX_CUDA(cudaMemcpy(b->d_off, b->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+    VLX_CUDA(cudaMalloc(&b->d_nao, n * sizeof(int)));
+    VLX_CUDA(cudaMemcpy(b->d_nao, nao.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    VLX_CUDA(cudaMalloc(&b->d_acc, (size_t)std::max<long long>(b->off.back(), 1) * sizeof(double)));
+    *out = b.release();
+    return VLX_B200_OK;
+}
+
+int vlx_b200_batch_destroy(vlx_b200_batch* b)
+{
+    if (!b) return VLX_B200_OK;
+    cudaSetDevice(b->device);
+    batch_release_graph(b);
+    for (auto& t : b->merged)
+        if (t.d_items) cudaFree(t.d_items);
+    cudaFree(b->d_blocks);
+    cudaFree(b->d_mols);
+    cudaFree(b->d_off);
+    cudaFree(b->d_nao);
+    cudaFree(b->d_acc);
+    if (b->d_counters) cudaFree(b->d_counters);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return VLX_B200_OK;
+}
+
+int vlx_b200_batch_offsets(const vlx_b200_batch* b, long long* offsets)
+{
+    if (!b || !offsets) return fail(VLX_B200_ERR_ARGUMENT, "batch_offsets: null argument");
+    std::copy(b->off.begin(), b->off.end(), offsets);
+    return VLX_B200_OK;
+}
+
+int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int symmetric, const char* label,
+                              double xfac, double omega, int ith, double* d_focks, void* stream, int use_graph,
+                              vlx_b200_stats* stats)
+{
+    if (!b || !d_densities || !d_focks) return fail(VLX_B200_ERR_ARGUMENT, "batch_fock_build: null argument");
+    if (!std::isfinite(omega) || omega < 0.0) return fail(VLX_B200_ERR_ARGUMENT, "omega must be finite and >= 0");
+    VLX_CUDA(cudaSetDevice(b->device));
+    double cj = 0.0, ck = 0.0;
+    const bool rs = label_is_range_separated(label);
+    const bool known = label_weights(label, symmetric, xfac, &cj, &ck) && !(rs && omega == 0.0);
+    const double omega2 = rs ? omega * omega : 0.0;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+    TaskSet* ts = nullptr;
+    int rc = batch_tasks(b, ith, &ts);
+    if (rc) return rc;
+    if (b->mols_D != d_densities) {
+        // the kernels read D and the accumulator through these records; any
+        // earlier build that reads them has to finish first
+        VLX_CUDA(cudaDeviceSynchronize());
+        std::vector<vlx::MolDev> h(b->mols.size());
+        for (size_t k = 0; k < h.size(); k++) {
+            const vlx_b200_screener* s = b->mols[k];
+            h[k].D = d_densities + b->off[k];
+            h[k].F = b->d_acc + b->off[k];
+            h[k].nao = s->nao;
+            for (int l = 0; l <= VLX_LMAX; l++) h[k].nl[l] = s->nl[l];
+        }
+        VLX_CUDA(cudaMemcpy(b->d_mols, h.data(), h.size() * sizeof(vlx::MolDev), cudaMemcpyHostToDevice));
+        b->mols_D = d_densities;
+    }
+    long long launches = 0;
+    if (!use_graph) {
+        rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_focks, st, &launches);
+        if (rc) return rc;
+    } else {
+        const bool same = b->exec && b->key_D == d_densities && b->key_F == d_focks && b->key_sym == symmetric &&
+                          b->key_ith == ith && b->key_cj == cj && b->key_ck == ck && b->key_om2 == omega2;
+        if (!same) {
+            VLX_CUDA(cudaStreamSynchronize(b->stream));
+            batch_release_graph(b);
+            cudaGraph_t graph = nullptr;
+            VLX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+            rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_focks, b->stream, &launches);
+            const cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
+            if (rc) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (ec != cudaSuccess) return fail(VLX_B200_ERR_CUDA, std::string("batch graph capture: ") +
+                                                                       cudaGetErrorString(ec));
+            const cudaError_t ei = cudaGraphInstantiate(&b->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) {
+                b->exec = nullptr;
+                return fail(VLX_B200_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ei));
+            }
+            b->key_D = d_densities;
+            b->key_F = d_focks;
+            b->key_sym = symmetric;
+            b->key_ith = ith;
+            b->key_cj = cj;
+            b->key_ck = ck;
+            b->key_om2 = omega2;
+            b->launches = launches;
+        }
+        launches = b->launches;
+        VLX_CUDA(cudaGraphLaunch(b->exec, st));
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->shell_quartets = known ? ts->quartets : 0;
+        stats->prim_quartets = known ? ts->prim_quartets : 0;
+        stats->kernel_launches = launches;
+    }
     return VLX_B200_OK;
 }
 

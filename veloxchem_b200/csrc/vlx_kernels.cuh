@@ -34,13 +34,13 @@ __device__ __forceinline__ void addF(double* F, int nao, int r, int c, double v)
 template <int NA, int NB, int NC, int ND, int MODE>
 __device__ __forceinline__ void digest(const double* f, const double s, const int lane, const int p0, const int nlp,
                                        const int q0, const int nlq, const int r0, const int nlr, const int s0,
-                                       const int nls, const FockArgs& a)
+                                       const int nls, const MolDev& m, const double cjw, const double ckw)
 {
-    const double* __restrict__ D = a.D;
-    double* F = a.F;
-    const int nao = a.nao;
-    const double cj = a.cj * s, ck = a.ck * s;
-    if (a.cj != 0.0) {
+    const double* __restrict__ D = m.D;
+    double* F = m.F;
+    const int nao = m.nao;
+    const double cj = cjw * s, ck = ckw * s;
+    if (cjw != 0.0) {
         // F_PQ: reduce over the lanes (ket pairs), then one atomic per element
 #pragma unroll
         for (int i = 0; i < NA; i++) {
@@ -85,7 +85,7 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
             }
         }
     }
-    if (a.ck != 0.0 && s != 0.0) {
+    if (ckw != 0.0 && s != 0.0) {
         // F_PR += sum_{j l} f D_QS ; F_RP (general) += sum f D_SQ
 #pragma unroll
         for (int i = 0; i < NA; i++) {
@@ -198,7 +198,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
     using C = EriClass<LA, LB, LC, LD>;
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
     const int lane = threadIdx.x & 31;
-    const int nlp = a.nl[LA], nlq = a.nl[LB], nlr = a.nl[LC], nls = a.nl[LD];
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(a.counter, 1);
@@ -208,6 +207,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
         const int bbi = w.blocks & 0xffff, kbi = w.blocks >> 16;
         const PairBlockDev bb = a.blocks[bbi];
         const PairBlockDev kb = a.blocks[kbi];
+        const MolDev m = a.mols ? a.mols[bb.mol] : a.mol;
+        const int nlp = m.nl[LA], nlq = m.nl[LB], nlr = m.nl[LC], nls = m.nl[LD];
         const PairView bra = make_view(bb, w.bra);
         const int p0 = __ldg(bb.ao + w.bra), q0 = __ldg(bb.ao + bb.npairs + w.bra);
         const double s_bra = (p0 == q0) ? 0.5 : 1.0;
@@ -219,24 +220,24 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
             double f[C::NSPH];
             if (mode & MODE_F32) {
                 float g[C::NSPH];
-                C::compute_f32(bra, ket, a.boys_f, g);
+                C::compute_f32(bra, ket, a.boys_f, (float)a.omega2, g);
 #pragma unroll
                 for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
             } else {
-                C::compute(bra, ket, a.boys, f);
+                C::compute(bra, ket, a.boys, a.omega2, f);
             }
             const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
             const int dmode = mode & 3;
             if (dmode == MODE_ERI) {
-                if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, a.nao);
+                if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, m.nao);
             } else {
                 double s = act ? s_bra : 0.0;
                 if (r0 == s0) s *= 0.5;
                 if (bbi == kbi && jj == w.bra) s *= 0.5;
                 if (dmode == MODE_FOCK_SYM)
-                    digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);
+                    digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
                 else
-                    digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, a);
+                    digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
             }
         }
     }
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const PairBlockDev* blocks,
     if (i >= b.npairs) return;
     const PairView v = make_view(b, i);
     double f[C::NSPH];
-    C::compute(v, v, boys, f);
+    C::compute(v, v, boys, 0.0, f);
     double mx = 0.0;
     for (int t = 0; t < C::NSPH; t++) mx = (f[t] > mx) ? f[t] : mx;
     maxv[i] = mx;

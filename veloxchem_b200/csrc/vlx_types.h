@@ -33,6 +33,7 @@ struct PairBlockDev {
     int npairs;
     int kprim;
     int la, lb;
+    int mol;             // molecule of the block in a batched build (index into FockArgs::mols)
 };
 
 // A run of ket pairs for one bra pair of one (bra block, ket block) job.
@@ -48,6 +49,14 @@ enum KernelMode { MODE_FOCK_SYM = 0, MODE_FOCK_GEN = 1, MODE_ERI = 2 };
 // the FP32 recursion (digestion and accumulation stay FP64)
 constexpr int MODE_F32 = 4;
 
+// Per-molecule data of a build: density, accumulator, basis dimensions.
+struct MolDev {
+    const double* D;          // density, nao x nao row-major
+    double* F;                // accumulator, nao x nao row-major
+    int nao;
+    int nl[VLX_LMAX + 1];     // shells per angular momentum (AO stride of component m)
+};
+
 struct FockArgs {
     const PairBlockDev* blocks;
     const WorkItem* items;
@@ -55,12 +64,11 @@ struct FockArgs {
     int* counter;             // work-queue head for this launch (zeroed before)
     const double* boys;       // Chebyshev table
     const float* boys_f;      // the same table rounded to float (mixed precision)
-    const double* D;          // density, nao x nao row-major
-    double* F;                // accumulator, nao x nao row-major
-    double* eri;              // MODE_ERI: nao^4 tensor
-    int nao;
-    int nl[VLX_LMAX + 1];     // shells per angular momentum (AO stride of component m)
+    MolDev mol;               // the molecule of a single build
+    const MolDev* mols;       // batched build: per molecule, indexed by PairBlockDev::mol (nullptr: single)
+    double* eri;              // MODE_ERI: nao^4 tensor of mol
     double cj, ck;            // J and K weights of the label
+    double omega2;            // 0: Coulomb; > 0: erf(omega r)/r with omega^2 (labels j_rs, k_rs, kx_rs)
 };
 
 }  // namespace vlx

@@ -67,6 +67,17 @@ def random_density(nao, nocc, seed):
     return q @ q.T
 
 
+def batch_clusters(count=256, nmax=16, seed=7, lattice=(3, 3, 2)):
+    """``count`` independent water clusters for batched builds: cluster i has
+    n_i ~ U{1..nmax} waters on the first n_i sites of ``lattice`` (x fastest)
+    and geometry seed ``seed + 1 + i``; returns (molecules, n_i list)."""
+    if nmax > lattice[0] * lattice[1] * lattice[2]:
+        raise ValueError('batch_clusters: lattice too small for nmax')
+    rng = np.random.default_rng(seed)
+    ns = [int(v) for v in rng.integers(1, nmax + 1, size=count)]
+    return [water_cluster(lattice, seed + 1 + i, n) for i, n in enumerate(ns)], ns
+
+
 # Named workloads (lattice, seed).
 CLUSTERS = {
     'h2o4': ((2, 2, 1), 1),
