@@ -1,0 +1,95 @@
+"""Host logic of the learned guess: the AO rotation of the reference's real
+solid harmonics (checked on the compiled reference's overlap matrix of a
+rotated molecule), invariance of the pair descriptors and local-frame
+blocks under rigid motions, and the block cut / assemble round trip."""
+
+import numpy as np
+import pytest
+
+from oracle.oracle import RefOracle, ref_available
+
+
+def _cluster(n=3, seed=4):
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200.geometry import water_cluster
+    mol = water_cluster((3, 3, 2), seed, n)
+    return mol, MolecularBasis.read(mol, 'def2-svp')
+
+
+def _moved(mol, Q, t):
+    from veloxchem_b200 import Molecule
+    from veloxchem_b200.guess import BOHR_IN_ANGSTROM
+    xyz = mol.get_coordinates_in_bohr() * BOHR_IN_ANGSTROM
+    return Molecule(mol.get_element_ids(), xyz @ Q.T + t, 'angstrom')
+
+
+def _full_rotation(lay, Q):
+    from veloxchem_b200.guess import atom_rotation
+    R = np.zeros((lay.nao, lay.nao))
+    for a in range(len(lay.z)):
+        R[np.ix_(lay.atom_aos[a], lay.atom_aos[a])] = atom_rotation(lay.atom_ls[a], Q)
+    return R
+
+
+Q0 = np.linalg.qr(np.random.default_rng(8).standard_normal((3, 3)))[0]
+Q0 = Q0 * np.sign(np.linalg.det(Q0))
+
+
+def test_sh_rotation_is_orthogonal_representation():
+    from veloxchem_b200.guess import sh_rotation
+    Q1 = np.linalg.qr(np.random.default_rng(1).standard_normal((3, 3)))[0]
+    Q1 *= np.sign(np.linalg.det(Q1))
+    for l in (0, 1, 2):
+        D = sh_rotation(l, Q0)
+        assert np.allclose(D @ D.T, np.eye(2 * l + 1), atol=1e-12)
+        assert np.allclose(sh_rotation(l, Q0 @ Q1), sh_rotation(l, Q0) @ sh_rotation(l, Q1), atol=1e-12)
+
+
+@pytest.mark.skipif(not ref_available(), reason='reference oracle not built')
+def test_overlap_of_rotated_molecule_transforms_by_ao_rotation():
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200.guess import ClusterLayout
+    mol, bas = _cluster(2)
+    mol2 = _moved(mol, Q0, np.array([0.3, -1.2, 2.0]))
+    bas2 = MolecularBasis.read(mol2, 'def2-svp')
+    S = RefOracle(mol, bas, partition=False).one_electron(0)
+    S2 = RefOracle(mol2, bas2, partition=False).one_electron(0)
+    R = _full_rotation(ClusterLayout(mol, bas), Q0)
+    assert np.max(np.abs(S2 - R @ S @ R.T)) < 1e-12
+
+
+def test_descriptors_and_blocks_invariant_under_rigid_motion():
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200.guess import ClusterLayout
+    mol, bas = _cluster(4)
+    mol2 = _moved(mol, Q0, np.array([1.0, 2.0, -0.5]))
+    bas2 = MolecularBasis.read(mol2, 'def2-svp')
+    a, b = ClusterLayout(mol, bas), ClusterLayout(mol2, bas2)
+    assert np.array_equal(a.pairs, b.pairs)
+    assert np.max(np.abs(a.descriptors() - b.descriptors())) < 1e-5
+    rng = np.random.default_rng(2)
+    c = rng.standard_normal((a.nao, 20))
+    D = c @ c.T
+    D2 = _full_rotation(a, Q0) @ D @ _full_rotation(a, Q0).T
+    Ta, Ma = a.local_blocks(D)
+    Tb, Mb = b.local_blocks(D2)
+    assert np.array_equal(Ma, Mb)
+    assert np.max(np.abs(Ta - Tb)) < 1e-5 * np.max(np.abs(Ta))
+
+
+def test_blocks_round_trip():
+    from veloxchem_b200.guess import ClusterLayout
+    mol, bas = _cluster(2)
+    lay = ClusterLayout(mol, bas)
+    assert np.all(lay.dist[lay.pairs[:, 0], lay.pairs[:, 1]] <= 5.0)
+    rng = np.random.default_rng(5)
+    c = rng.standard_normal((lay.nao, 10))
+    D = c @ c.T
+    T, M = lay.local_blocks(D)
+    back = lay.assemble(T.astype(np.float64))
+    covered = np.zeros_like(D, dtype=bool)
+    for i, j in lay.pairs:
+        covered[np.ix_(lay.atom_aos[i], lay.atom_aos[j])] = True
+        covered[np.ix_(lay.atom_aos[j], lay.atom_aos[i])] = True
+    assert np.max(np.abs((back - D)[covered])) < 1e-5 * np.max(np.abs(D))
+    assert np.all(back[~covered] == 0.0)

@@ -9,8 +9,10 @@ scfrestdriver.py) for the parts a restricted HF energy needs:
   ``ovl_thresh`` = 1e-6 (scfdriver.py:1280-1300);
 * initial density: SAD (SadGuessDriver.compute, sadguessdriver.py:841-971)
   built from the minimal basis ``ao-start-guess`` with neutral-atom occupation
-  numbers (the reference also shifts them by dftd4/EEQ partial charges), or
-  the core-Hamiltonian guess;
+  numbers (the reference also shifts them by dftd4/EEQ partial charges), the
+  core-Hamiltonian guess, or ``'learned'`` (guess.LearnedGuessDriver, no
+  reference counterpart): the learned and the SAD densities both enter the
+  first iteration and the one with the lower energy is kept;
 * per iteration: F_2e = 2J - K from the device-resident Fock build with the
   reference's dynamic integral threshold (_get_dyn_threshold,
   scfdriver.py:2410-2435), energy terms e_ee = sum D F_2e, e_kin = 2 sum D T,
@@ -110,6 +112,7 @@ class ScfRestrictedDriver:
         self.eri_thresh = 1.0e-12
         self.ovl_thresh = 1.0e-6
         self.guess = 'sad'
+        self.guess_weights = None  # learned guess: network file (default: the shipped def2-SVP water model)
         # mixed precision: quartets with Schwarz bound x max|D| < fp32_cutoff in
         # FP32 while the electronic gradient is above fp32_until_grad; the
         # final iterations are FP64, so the converged energy is the FP64 one
@@ -154,16 +157,41 @@ class ScfRestrictedDriver:
             self.timings['screener_s'] = time.perf_counter() - t0
         if guess_density is not None:
             D = torch.as_tensor(np.asarray(guess_density), dtype=torch.float64, device=dev)
-        elif self.guess == 'sad':
+        elif self.guess in ('sad', 'learned'):
             if min_basis is None:
                 min_basis = MolecularBasis.read(molecule, 'ao-start-guess')
-            D = torch.from_numpy(SadGuessDriver().compute(molecule, min_basis, ao_basis, self.device)).to(dev)
+            D_sad = SadGuessDriver().compute(molecule, min_basis, ao_basis, self.device)
+            D = torch.from_numpy(D_sad).to(dev)
         else:
             e, c = torch.linalg.eigh(X.T @ H @ X)
             C = X @ c[:, :nocc]
             D = C @ C.T
         stream = torch.cuda.current_stream(dev)
         F2e = torch.empty_like(D)
+
+        def build(dens, out, ith):
+            nat.check(nat.lib().vlx_b200_fock_build_device(screener.handle, ctypes.c_void_p(dens.data_ptr()), 1,
+                                                            b'2jk', 1.0, 0.0, ith, ctypes.c_void_p(out.data_ptr()),
+                                                            ctypes.c_void_p(stream.cuda_stream)), 'fock_build')
+
+        first = None  # (F2e) of the first iteration, when the guess selection already built it
+        self.guess_used = self.guess if guess_density is None else 'given'
+        if guess_density is None and self.guess == 'learned':
+            from .guess import LearnedGuessDriver
+            t0 = time.perf_counter()
+            D_l = LearnedGuessDriver(self.guess_weights, self.device).predict(molecule, ao_basis, D_sad,
+                                                                             S.cpu().numpy(), nocc)
+            self.timings['learned_guess_s'] = time.perf_counter() - t0
+            ith0 = int(-math.log10(self.dyn_threshold(1.0)))
+            cands = []
+            for name, dens in (('learned', torch.from_numpy(D_l).to(dev)), ('sad', D)):
+                dens = 0.5 * (dens + dens.T).contiguous()
+                f2 = torch.empty_like(dens)
+                build(dens, f2, ith0)
+                cands.append((float(torch.sum(dens * f2) + 2.0 * torch.sum(dens * H)), name, dens, f2))
+            torch.cuda.synchronize(dev)
+            e_best, self.guess_used, D, first = min(cands, key=lambda c: c[0])
+            self.timings['guess_energies'] = {c[1]: c[0] + e_nuc for c in cands}
         focks, errs = [], []
         e_grad, energy, e_old = 1.0, 0.0, 0.0
         self.history = []
@@ -178,9 +206,11 @@ class ScfRestrictedDriver:
             else:
                 screener.set_fp32_threshold(0.0, 0.0)
             t0 = time.perf_counter()
-            nat.check(nat.lib().vlx_b200_fock_build_device(screener.handle, ctypes.c_void_p(D.data_ptr()), 1, b'2jk',
-                                                            1.0, 0.0, ith, ctypes.c_void_p(F2e.data_ptr()),
-                                                            ctypes.c_void_p(stream.cuda_stream)), 'fock_build')
+            if first is not None:
+                F2e.copy_(first)
+                first = None
+            else:
+                build(D, F2e, ith)
             torch.cuda.synchronize(dev)
             fock_ms += 1e3 * (time.perf_counter() - t0)
             e_ee = torch.sum(D * F2e)
@@ -212,7 +242,8 @@ class ScfRestrictedDriver:
         return {'scf_energy': energy, 'converged': converged, 'iterations': len(self.history),
                 'e_grad': e_grad, 'nuclear_repulsion': e_nuc, 'D_alpha': D.cpu().numpy(),
                 'C_alpha': (X @ c).cpu().numpy(), 'E_alpha': e.cpu().numpy(), 'F_alpha': F.cpu().numpy(),
-                'history': self.history, 'timings': dict(self.timings), 'screener': screener}
+                'history': self.history, 'timings': dict(self.timings), 'screener': screener,
+                'guess_used': self.guess_used}
 
     @staticmethod
     def _diis(focks, errs):
