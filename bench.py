@@ -247,7 +247,8 @@ def run_ours(args):
     all_flops = sum(p['flops'] for p in prof)
     roofline = {'bound': 'fp64', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
                 'traffic': _profiled_traffic(top),
-                'kernel': 'quartet_kernel<%d,%d,%d,%d>' % (top['la'], top['lb'], top['lc'], top['ld']),
+                'kernel': ('coop_quartet_kernel<double,%d,%d,%d,%d>' if top['table_driven'] else
+                           'quartet_kernel<%d,%d,%d,%d>') % (top['la'], top['lb'], top['lc'], top['ld']),
                 'kernel_share': top['device_ms'] / tot_prof_ms,
                 'peak_source': 'measured: FP64 FMA-chain probe kernel (vlx_b200_fp64_peak), burst; '
                                'MEASURED_PEAKS.json has no FP64 figure',

@@ -160,8 +160,8 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_den
  * whose Schwarz bound sqrt((ab|ab)) sqrt((cd|cd)) times max_abs_density is
  * below `cutoff` (decided on the decade bins: bound <= 10^-(bin_ab + bin_cd))
  * are evaluated with the FP32 recursion; digestion and the Fock accumulator
- * stay FP64.  Classes served by the warp-cooperative kernel stay FP64.
- * cutoff <= 0 switches it off (the default).  No counterpart in the
+ * stay FP64 (both the compiled classes and the warp-cooperative classes have
+ * an FP32 twin).  cutoff <= 0 switches it off (the default).  No counterpart in the
  * reference (its Fock build is FP64 throughout). */
 int vlx_b200_set_fp32_threshold(vlx_b200_screener* screener, double cutoff, double max_abs_density);
 

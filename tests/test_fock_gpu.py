@@ -250,6 +250,9 @@ def test_mixed_precision_build():
         prof = nat.fock_profile(s, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
         n32 = sum(p['fp32_quartets'] for p in prof)
         assert n32 > 0
+        if cutoff >= 1e-7:  # both kernel families evaluate FP32 quartets
+            assert any(p['fp32_quartets'] > 0 for p in prof if p['table_driven'])
+            assert any(p['fp32_quartets'] > 0 for p in prof if not p['table_driven'])
         errors[cutoff] = float((fm - f64).abs().max())
     assert errors[1e-9] < 1e-10 and errors[1e-7] < 1e-8 and errors[1e-5] < 1e-6
     s.set_fp32_threshold(0.0, 0.0)

@@ -37,7 +37,8 @@ def nvcc():
 def _headers_digest():
     h = hashlib.sha256()
     for p in sorted(list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) +
-                    [GEN / 'dispatch.inc', GEN / 'sph_table.inc', INCLUDE / 'vlx_b200.h']):
+                    [GEN / 'dispatch.inc', GEN / 'sph_table.inc', GEN / 'xform.inc', GEN / 'coop_classes.inc',
+                     INCLUDE / 'vlx_b200.h']):
         if p.exists():
             h.update(p.read_bytes())
     h.update(' '.join(NVCC_FLAGS).encode())

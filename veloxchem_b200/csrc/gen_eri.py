@@ -649,6 +649,139 @@ def emit_sph_table(outdir, lmax=4):
         path.write_text(text)
 
 
+def _lin_expr(terms):
+    """sum of (coefficient, name) terms as T-typed code ('T(0)' if empty)."""
+    parts = ['T(%s) * %s' % (_num(c), n) for c, n in terms if c != 0.0]
+    return ' + '.join(parts) if parts else 'T(0)'
+
+
+def ket_xform_code(lc, ld):
+    """Ket half of the post-contraction steps for one bra component e: ket
+    HRR |c+1_i, d) = |c, d+1_i) + (D_i - C_i)|c, d) on the Cartesian f-vector
+    [e 0 | f 0], f in [ld, lc+ld] (input in[jf], f_targets order), then the
+    ket Cartesian -> spherical transform; output out[(k nd + l) os]."""
+    f_t = [c for l in range(ld, lc + ld + 1) for c in cart_list(l)]
+    f_index = {f: j for j, f in enumerate(f_t)}
+    nodes, order = {}, []
+
+    def need(c, d):
+        key = (c, d)
+        if key in nodes:
+            return key
+        if sum(c) == 0:
+            nodes[key] = ('F', f_index[d])
+        else:
+            i = pick_axis(c)
+            c1 = sub1(c, i)
+            nodes[key] = ('H', i, need(c1, add1(d, i)), need(c1, d))
+        order.append(key)
+        return key
+
+    cc, dc = cart_list(lc), cart_list(ld)
+    for c in cc:
+        for d in dc:
+            need(c, d)
+    names = {}
+    body = []
+    for n_, key in enumerate(order):
+        node = nodes[key]
+        nm = 'k%d' % n_
+        names[key] = nm
+        if node[0] == 'F':
+            body.append('        const T %s = in[%d];' % (nm, node[1]))
+        else:
+            body.append('        const T %s = %s + DC%s * %s;' % (nm, names[node[2]], AX[node[1]], names[node[3]]))
+    sc, sd = sph_coefficients(lc), sph_coefficients(ld)
+    nc, nd = 2 * lc + 1, 2 * ld + 1
+    for k in range(nc):
+        for l in range(nd):
+            terms = [(sc[k][ic] * sd[l][jd], names[(c, d)]) for ic, c in enumerate(cc) for jd, d in enumerate(dc)
+                     if sc[k][ic] != 0.0 and sd[l][jd] != 0.0]
+            body.append('        out[%d * os] = %s;' % (k * nd + l, _lin_expr(terms)))
+    head = ['template <> struct KetXform<%d, %d> {' % (lc, ld),
+            '    static constexpr int NIN = %d, NOUT = %d;' % (len(f_t), nc * nd),
+            '    template <typename T>',
+            '    __device__ __forceinline__ static void run(const T* __restrict__ in, T* __restrict__ out, const int os,',
+            '                                               const T DCx, const T DCy, const T DCz)',
+            '    {',
+            '        (void)DCx; (void)DCy; (void)DCz;']
+    return '\n'.join(head + body + ['    }', '};', ''])
+
+
+def bra_xform_code(la, lb):
+    """Bra half for one half-spherical ket component: bra HRR
+    (a+1_i, b| = (a, b+1_i| + (B_i - A_i)(a, b| on the e-vector, e in
+    [lb, la+lb] (input in[ie is], e_targets order), then the bra Cartesian ->
+    spherical transform; output out[(i nb + j) os]."""
+    e_t = [c for l in range(lb, la + lb + 1) for c in cart_list(l)]
+    e_index = {e: j for j, e in enumerate(e_t)}
+    nodes, order = {}, []
+
+    def need(a, b):
+        key = (a, b)
+        if key in nodes:
+            return key
+        if sum(a) == 0:
+            nodes[key] = ('E', e_index[b])
+        else:
+            i = pick_axis(a)
+            a1 = sub1(a, i)
+            nodes[key] = ('H', i, need(a1, add1(b, i)), need(a1, b))
+        order.append(key)
+        return key
+
+    ac, bc = cart_list(la), cart_list(lb)
+    for a in ac:
+        for b in bc:
+            need(a, b)
+    names = {}
+    body = []
+    for n_, key in enumerate(order):
+        node = nodes[key]
+        nm = 'b%d' % n_
+        names[key] = nm
+        if node[0] == 'E':
+            body.append('        const T %s = in[%d * is];' % (nm, node[1]))
+        else:
+            body.append('        const T %s = %s + BA%s * %s;' % (nm, names[node[2]], AX[node[1]], names[node[3]]))
+    sa, sb = sph_coefficients(la), sph_coefficients(lb)
+    na, nb = 2 * la + 1, 2 * lb + 1
+    for i in range(na):
+        for j in range(nb):
+            terms = [(sa[i][ia] * sb[j][jb], names[(a, b)]) for ia, a in enumerate(ac) for jb, b in enumerate(bc)
+                     if sa[i][ia] != 0.0 and sb[j][jb] != 0.0]
+            body.append('        out[%d * os] = %s;' % (i * nb + j, _lin_expr(terms)))
+    head = ['template <> struct BraXform<%d, %d> {' % (la, lb),
+            '    static constexpr int NIN = %d, NOUT = %d;' % (len(e_t), na * nb),
+            '    template <typename T>',
+            '    __device__ __forceinline__ static void run(const T* __restrict__ in, const int is, T* __restrict__ out,',
+            '                                               const int os, const T BAx, const T BAy, const T BAz)',
+            '    {',
+            '        (void)BAx; (void)BAy; (void)BAz;']
+    return '\n'.join(head + body + ['    }', '};', ''])
+
+
+def emit_xforms(outdir, lmax, interp):
+    """xform.inc: the compiled ket / bra transforms of every pair class, and
+    coop_classes.inc: one VLX_COOP_CLASS(la, lb, lc, ld) line per
+    warp-cooperative class."""
+    out = ['// generated by gen_eri.py: post-contraction transforms (HRR + Cartesian -> spherical)',
+           'template <int LC, int LD> struct KetXform;', 'template <int LA, int LB> struct BraXform;', '']
+    for a, b in pair_classes(lmax):
+        out.append(ket_xform_code(a, b))
+        out.append(bra_xform_code(a, b))
+    text = '\n'.join(out)
+    path = outdir / 'xform.inc'
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+    lines = ['// generated by gen_eri.py: warp-cooperative quartet classes'] + \
+            ['VLX_COOP_CLASS(%d, %d, %d, %d)' % c for c in interp]
+    text = '\n'.join(lines) + '\n'
+    path = outdir / 'coop_classes.inc'
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+
+
 def main():
     outdir = Path(sys.argv[1])
     lmax = int(sys.argv[2]) if len(sys.argv) > 2 else 3
@@ -663,6 +796,7 @@ def main():
         emit_class_file(cls, outdir)
     emit_dispatch(compiled, lmax, outdir)
     emit_sph_table(outdir)
+    emit_xforms(outdir, lmax, interp)
     import gen_coop
     gen_coop.emit_blob(interp, outdir / 'coop_programs.bin')
     for p in outdir.glob('class_*.cu'):

@@ -302,7 +302,7 @@ struct ClassTasks {
     int coop = -1;      // index into DeviceGlobals::coop
     int la = 0, lb = 0, lc = 0, ld = 0;
     std::vector<WorkItem> items;    // FP64 quartets
-    std::vector<WorkItem> items32;  // FP32 quartets (mixed precision, compiled classes only)
+    std::vector<WorkItem> items32;  // FP32 quartets (mixed precision)
     size_t offset = 0, offset32 = 0;
     long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0, fp32_quartets = 0;
 };
@@ -479,8 +479,8 @@ int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
         if (!done && n > 0) {
             const int ic = find_coop(s->glob, pb.la, pb.lb, pb.la, pb.lb);
             if (ic < 0) return fail(VLX_B200_ERR_UNSUPPORTED, "no kernel for Schwarz class");
-            vlx::launch_coop_schwarz(s->d_blocks, (int)b, n, s->glob->coop[ic], s->glob->boys, d_max[b],
-                                     s->glob->nsm, s->stream);
+            VLX_CUDA(vlx::launch_coop_schwarz(s->d_blocks, (int)b, n, s->glob->coop[ic], s->glob->boys, d_max[b],
+                                              s->glob->nsm, s->stream));
         }
         VLX_CUDA(cudaGetLastError());
     }
@@ -555,7 +555,7 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                     // 10^-(bin_bra + bin_ket) times max|D| is below the FP32 cutoff
                     // are the tail [k_mid, k1) of the run
                     int k_mid = k1;
-                    if (s->ith32 >= 0 && ct.compiled >= 0) {
+                    if (s->ith32 >= 0) {
                         const int b32 = s->ith32 - bx;
                         const int kb32 = (b32 <= 0) ? 0 : Pk.bin_off[std::min(b32, 16)];
                         k_mid = std::min(k1, std::max(k0, kb32));
@@ -707,11 +707,19 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
             }
         } else {
             const CoopClassDev& cc = L.glob->coop[ct.coop];
-            const int wpb = vlx::coop_warps_per_block(cc);
-            const int cap = vlx::coop_blocks_per_sm(cc) * nsm;
-            const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
-            vlx::launch_coop_quartet(mode, a, cc, grid, st);
-            if (launches) (*launches)++;
+            for (int f = 0; f < 2; f++) {
+                const std::vector<WorkItem>& its = f ? ct.items32 : ct.items;
+                if (its.empty()) continue;
+                FockArgs ac = a;
+                ac.items = ts->d_items + (f ? ct.offset32 : ct.offset);
+                ac.nitems = (int)its.size();
+                ac.counter = L.counters + (f ? ts->classes.size() : 0) + c;
+                const int wpb = vlx::coop_warps_per_block(cc, f != 0);
+                const int cap = vlx::coop_blocks_per_sm(cc, f != 0) * nsm;
+                const int grid = std::max(1, std::min((int)((its.size() + wpb - 1) / wpb), cap));
+                VLX_CUDA(vlx::launch_coop_quartet(f ? (mode | vlx::MODE_F32) : mode, ac, cc, grid, st));
+                if (launches) (*launches)++;
+            }
         }
         VLX_CUDA(cudaGetLastError());
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].second, st));
@@ -1173,7 +1181,7 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
                 const int wpb = vlx::coop_warps_per_block(cc);
                 const int cap = vlx::coop_blocks_per_sm(cc) * s->glob->nsm;
                 const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
-                vlx::launch_coop_quartet(mode, a, cc, grid, st);
+                VLX_CUDA(vlx::launch_coop_quartet(mode, a, cc, grid, st));
             }
             VLX_CUDA(cudaGetLastError());
         }

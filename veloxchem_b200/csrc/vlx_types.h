@@ -45,7 +45,7 @@ struct WorkItem {
 };
 
 enum KernelMode { MODE_FOCK_SYM = 0, MODE_FOCK_GEN = 1, MODE_ERI = 2 };
-// or-ed into the mode of a compiled-class launch: evaluate the quartets with
+// or-ed into the mode of a class launch: evaluate the quartets with
 // the FP32 recursion (digestion and accumulation stay FP64)
 constexpr int MODE_F32 = 4;
 

@@ -1,0 +1,198 @@
+"""Measurement workloads beyond the single-build bench line.
+
+    python -m veloxchem_b200.workloads c3 [--out FILE]     # (H2O)64 / def2-TZVP builds and SCF
+    python -m veloxchem_b200.workloads c4 [--out FILE]     # 256 small clusters, batched builds
+    python -m veloxchem_b200.workloads c2scf [--out FILE]  # (H2O)32 / def2-SVP SCF, plain and mixed
+
+Each prints one JSON object (and writes it to --out).  Times are CUDA-event
+device times for builds and wall-clock times for SCF runs (which include the
+host-side linear algebra and synchronisation of the driver).
+"""
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _cluster(name, basis):
+    from . import MolecularBasis
+    from .geometry import CLUSTERS, water_cluster
+    lat, seed = CLUSTERS[name]
+    mol = water_cluster(lat, seed)
+    return mol, MolecularBasis.read(mol, basis)
+
+
+def _build_ms(scr, d, f, reps=3):
+    """Device time (ms, best of reps) of one 2J-K build at ithreshold 12."""
+    import ctypes
+    from . import _native as nat
+    torch = _torch()
+    st = torch.cuda.Stream()
+    best = 1e30
+    with torch.cuda.stream(st):
+        for _ in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            nat.check(nat.lib().vlx_b200_fock_build_device(scr.handle, ctypes.c_void_p(d.data_ptr()), 1, b'2jk', 1.0,
+                                                            0.0, 12, ctypes.c_void_p(f.data_ptr()),
+                                                            ctypes.c_void_p(st.cuda_stream)), 'fock_build')
+            e1.record(st)
+            st.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
+    from . import T4CScreener
+    from . import _native as nat
+    from .geometry import random_density
+    from .scf import ScfRestrictedDriver
+    torch = _torch()
+    mol, bas = _cluster('h2o64', 'def2-tzvp')
+    scr = T4CScreener()
+    scr.partition(bas, mol, 'eri')
+    d = torch.from_numpy(random_density(scr.nao, 320, 1)).cuda()
+    f64 = torch.empty_like(d)
+    out = {'workload': '(H2O)64 / def2-TZVP, 2J-K, ithreshold 12', 'nao': scr.nao}
+    t64 = _build_ms(scr, d, f64)
+    prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
+    flops = sum(p['flops'] for p in prof)
+    out['fp64'] = {'build_ms': t64, 'flops': flops, 'tflops': flops / t64 / 1e9,
+                   'classes': sorted([{'cls': '%d%d%d%d' % (p['la'], p['lb'], p['lc'], p['ld']),
+                                       'table_driven': p['table_driven'], 'ms': p['device_ms'],
+                                       'quartets': p['shell_quartets'], 'prim_quartets': p['prim_quartets'],
+                                       'tflops': p['flops'] / max(p['device_ms'], 1e-9) / 1e9} for p in prof],
+                                     key=lambda r: -r['ms'])[:20]}
+    dmax = float(d.abs().max())
+    out['mixed'] = []
+    for cut in cutoffs:
+        scr.set_fp32_threshold(cut, dmax)
+        fm = torch.empty_like(d)
+        tm = _build_ms(scr, d, fm)
+        prof = nat.fock_profile(scr, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
+        n32 = sum(p['fp32_quartets'] for p in prof)
+        nq = sum(p['shell_quartets'] for p in prof)
+        out['mixed'].append({'cutoff': cut, 'build_ms': tm, 'speedup': t64 / tm, 'fp32_share': n32 / max(nq, 1),
+                             'max_abs_fock_error': float((fm - f64).abs().max())})
+    scr.set_fp32_threshold(0.0, 0.0)
+    if scf:
+        runs = {}
+        for name, cut in (('fp64', 0.0), ('mixed_1e-6', 1e-6)):
+            drv = ScfRestrictedDriver()
+            drv.fp32_cutoff = cut
+            t0 = time.perf_counter()
+            res = drv.compute(mol, bas, screener=scr)
+            runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
+                          'converged': res['converged'], 'wall_s': time.perf_counter() - t0,
+                          'fock_ms_total': res['timings']['fock_ms_total'],
+                          'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
+                                      for h in res['history']]}
+        e_ref = runs['fp64']['energy']
+        for r in runs.values():
+            r['energy_error'] = r['energy'] - e_ref
+            r['time_to_1e-6_s'] = next((h[3] for k, h in enumerate(r['history'])
+                                        if all(abs(x[1] - e_ref) < 1e-6 for x in r['history'][k:])), None)
+        out['scf'] = runs
+    return out
+
+
+def c4(count=256, nmax=16, reps=5):
+    from . import MolecularBasis, T4CScreener
+    from .batch import FockBatch
+    from .geometry import batch_clusters, random_density
+    torch = _torch()
+    mols, ns = batch_clusters(count, nmax, 7)
+    scrs, dens = [], []
+    for i, (m, n) in enumerate(zip(mols, ns)):
+        b = MolecularBasis.read(m, 'def2-svp')
+        s = T4CScreener()
+        s.partition(b, m, 'eri')
+        scrs.append(s)
+        dens.append(random_density(s.nao, 5 * n, 1000 + i))
+    batch = FockBatch(scrs)
+    d = torch.from_numpy(batch.pack(dens)).cuda()
+    f = torch.empty_like(d)
+    st = torch.cuda.Stream()
+    res = {'workload': '%d water clusters, n ~ U{1..%d}, def2-SVP, 2J-K, ithreshold 12' % (count, nmax),
+           'nao_total': int(sum(s.nao for s in scrs)), 'nao_range': [min(s.nao for s in scrs),
+                                                                    max(s.nao for s in scrs)]}
+    with torch.cuda.stream(st):
+        for graph in (True, False):
+            batch.build_device(d, f, stream=st, use_graph=graph)
+            st.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                batch.build_device(d, f, stream=st, use_graph=graph)
+            e1.record(st)
+            st.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res['batched_graph' if graph else 'batched_nograph'] = {
+                'ms_per_batch': ms, 'builds_per_s': count / (ms * 1e-3),
+                'kernel_launches': batch.last_stats['kernel_launches']}
+        # one molecule per call through the single-molecule entry point
+        import ctypes
+        from . import _native as nat
+        fs = [torch.empty((s.nao, s.nao), dtype=torch.float64, device='cuda') for s in scrs]
+        ds = [d[batch.offsets[k]:batch.offsets[k + 1]].view(s.nao, s.nao) for k, s in enumerate(scrs)]
+        for k, s in enumerate(scrs):  # work lists
+            nat.check(nat.lib().vlx_b200_fock_build_device(s.handle, ctypes.c_void_p(ds[k].data_ptr()), 1, b'2jk',
+                                                            1.0, 0.0, 12, ctypes.c_void_p(fs[k].data_ptr()),
+                                                            ctypes.c_void_p(st.cuda_stream)), 'fock_build')
+        st.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for k, s in enumerate(scrs):
+            nat.check(nat.lib().vlx_b200_fock_build_device(s.handle, ctypes.c_void_p(ds[k].data_ptr()), 1, b'2jk',
+                                                            1.0, 0.0, 12, ctypes.c_void_p(fs[k].data_ptr()),
+                                                            ctypes.c_void_p(st.cuda_stream)), 'fock_build')
+        e1.record(st)
+        st.synchronize()
+        ms = e0.elapsed_time(e1)
+        res['one_per_call'] = {'ms_per_batch': ms, 'builds_per_s': count / (ms * 1e-3)}
+    err = max(float((f[batch.offsets[k]:batch.offsets[k + 1]].view(s.nao, s.nao) - fs[k]).abs().max())
+              for k, s in enumerate(scrs))
+    res['max_abs_error_vs_single'] = err
+    return res
+
+
+def c2scf():
+    from .scf import ScfRestrictedDriver
+    mol, bas = _cluster('h2o32', 'def2-svp')
+    runs = {}
+    for name, cut in (('warmup', 0.0), ('fp64', 0.0), ('mixed_1e-6', 1e-6)):
+        drv = ScfRestrictedDriver()
+        drv.fp32_cutoff = cut
+        t0 = time.perf_counter()
+        res = drv.compute(mol, bas)
+        if name == 'warmup':
+            continue
+        runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
+                      'wall_s': time.perf_counter() - t0, 'fock_ms_total': res['timings']['fock_ms_total']}
+    runs['energy_error_mixed'] = runs['mixed_1e-6']['energy'] - runs['fp64']['energy']
+    return {'workload': '(H2O)32 / def2-SVP RHF from SAD, gradient < 1e-6', **runs}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument('which', choices=['c3', 'c4', 'c2scf'])
+    ap.add_argument('--out', default=None)
+    ap.add_argument('--no-scf', action='store_true')
+    a = ap.parse_args(argv)
+    res = c3(scf=not a.no_scf) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf())
+    text = json.dumps(res, indent=1)
+    if a.out:
+        with open(a.out, 'w') as fh:
+            fh.write(text)
+    print(text)
+
+
+if __name__ == '__main__':
+    main()
