@@ -167,12 +167,16 @@ class ScfRestrictedDriver:
             C = X @ c[:, :nocc]
             D = C @ C.T
         stream = torch.cuda.current_stream(dev)
+        # the builds run on torch's current stream; its default stream has
+        # handle 0, which the library would read as "its own stream", so the
+        # legacy default stream is passed explicitly (cudaStreamLegacy = 1)
+        sp = stream.cuda_stream or 1
         F2e = torch.empty_like(D)
 
         def build(dens, out, ith):
             nat.check(nat.lib().vlx_b200_fock_build_device(screener.handle, ctypes.c_void_p(dens.data_ptr()), 1,
                                                             b'2jk', 1.0, 0.0, ith, ctypes.c_void_p(out.data_ptr()),
-                                                            ctypes.c_void_p(stream.cuda_stream)), 'fock_build')
+                                                            ctypes.c_void_p(sp)), 'fock_build')
 
         first = None  # (F2e) of the first iteration, when the guess selection already built it
         self.guess_used = self.guess if guess_density is None else 'given'

@@ -165,18 +165,24 @@ def main(argv=None):
     ap.add_argument('--eval-waters', type=int, default=48)
     ap.add_argument('--eval-seed', type=int, default=900000)
     ap.add_argument('--report', default='guess_report.json')
+    ap.add_argument('--eval-only', default=None, help='evaluate this weights file, no training')
     a = ap.parse_args(argv)
 
     def log(msg):
         print(msg, flush=True)
 
-    t0 = time.perf_counter()
-    X, T, M, owner = generate(a.clusters, a.nmin, a.nmax, a.seed, log)
-    t_data = time.perf_counter() - t0
-    log('samples %d pairs from %d clusters, %.1f s' % (len(X), len(np.unique(owner)), t_data))
-    state, hist, t_train = train(X, T, M, owner, epochs=a.epochs, log=log)
-    np.savez(a.out, **state)
-    rows = evaluate(a.out, a.eval, a.eval_waters, a.eval_seed, log) if a.eval > 0 else []
+    if a.eval_only:
+        X, t_data, t_train, hist = np.zeros((0, 1)), 0.0, 0.0, []
+        weights = a.eval_only
+    else:
+        t0 = time.perf_counter()
+        X, T, M, owner = generate(a.clusters, a.nmin, a.nmax, a.seed, log)
+        t_data = time.perf_counter() - t0
+        log('samples %d pairs from %d clusters, %.1f s' % (len(X), len(np.unique(owner)), t_data))
+        state, hist, t_train = train(X, T, M, owner, epochs=a.epochs, log=log)
+        np.savez(a.out, **state)
+        weights = a.out
+    rows = evaluate(weights, a.eval, a.eval_waters, a.eval_seed, log) if a.eval > 0 else []
     summary = {}
     for name in ('sad', 'learned'):
         its = [r[name]['iters_to_1e-6'] for r in rows if r[name]['iters_to_1e-6']]
