@@ -93,3 +93,54 @@ def test_blocks_round_trip():
         covered[np.ix_(lay.atom_aos[j], lay.atom_aos[i])] = True
     assert np.max(np.abs((back - D)[covered])) < 1e-5 * np.max(np.abs(D))
     assert np.all(back[~covered] == 0.0)
+
+
+def _loop_descriptors(lay):
+    """Per-pair loop form of the descriptors (the form the shipped network was
+    trained with), to pin the vectorised implementation."""
+    import math
+    from veloxchem_b200.guess import ENV_CUTOFF, MOM_CENTERS, MOM_WIDTH, NFEAT, NTYPES, RBF_CENTERS, RBF_WIDTH
+
+    def env(i):
+        d = lay.dist[i]
+        mask = (d > 1e-8) & (d < ENV_CUTOFF)
+        out = []
+        for el in (8, 1):
+            sel = mask & (lay.z == el)
+            out.append(np.exp(-((d[sel][:, None] - RBF_CENTERS[None, :]) / RBF_WIDTH) ** 2).sum(axis=0))
+        v = (lay.xyz[mask] - lay.xyz[i]) / d[mask][:, None]
+        v = v @ lay.frames[lay.water[i]]
+        g = np.exp(-((d[mask][:, None] - MOM_CENTERS[None, :]) / MOM_WIDTH) ** 2)
+        out.append((g[:, :, None] * v[:, None, :]).sum(axis=0).ravel())
+        return np.concatenate(out)
+
+    e = [env(i) for i in range(len(lay.z))]
+    X = np.zeros((len(lay.pairs), NFEAT))
+    for p, (i, j) in enumerate(lay.pairs):
+        zi, zj = lay.z[i], lay.z[j]
+        t = (0 if zi == 8 else 1) if i == j else (2 if (zi == 8 and zj == 8) else (3 if zi == 8 else 4))
+        wa, wb = lay.water[i], lay.water[j]
+        Fa, Fb = lay.frames[wa], lay.frames[wb]
+        dv = lay.xyz[j] - lay.xyz[i]
+        d = lay.dist[i, j]
+        f = [np.eye(NTYPES)[t], [1.0 if wa == wb else 0.0], [d, math.exp(-d), 1.0 / (1.0 + d)], dv @ Fa, dv @ Fb,
+             (Fa.T @ Fb).ravel(), (lay.xyz[i] - lay.origin[wa]) @ Fa, (lay.xyz[j] - lay.origin[wb]) @ Fb, e[i], e[j]]
+        X[p] = np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in f])
+    return X
+
+
+def test_vectorised_layout_matches_pair_loop():
+    from veloxchem_b200.guess import ClusterLayout, atom_rotation
+    mol, bas = _cluster(6, seed=9)
+    lay = ClusterLayout(mol, bas)
+    assert np.max(np.abs(lay.descriptors() - _loop_descriptors(lay))) < 1e-5
+    for a in range(len(lay.z)):
+        assert np.allclose(lay.rot[a], atom_rotation(lay.atom_ls[a], lay.frames[lay.water[a]].T), atol=1e-12)
+    rng = np.random.default_rng(1)
+    c = rng.standard_normal((lay.nao, 12))
+    D = c @ c.T
+    T, M = lay.local_blocks(D)
+    for p, (i, j) in enumerate(lay.pairs):
+        blk = lay.rot[i] @ D[np.ix_(lay.atom_aos[i], lay.atom_aos[j])] @ lay.rot[j].T
+        assert np.allclose(T[p, :blk.size], blk.ravel(), atol=1e-5 * np.max(np.abs(D)))
+        assert M[p, :blk.size].all() and not M[p, blk.size:].any()

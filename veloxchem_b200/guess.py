@@ -90,7 +90,8 @@ def atom_rotation(shell_ls, Q):
 # ------------------------------------------------------------ structure of a cluster
 
 class ClusterLayout:
-    """Atoms, AO lists, water frames and the pair list of one water cluster."""
+    """Atoms, AO lists, water frames and the pair list of one water cluster
+    (all per-pair work vectorised over the pairs of one element pair)."""
 
     def __init__(self, molecule, basis):
         self.z = np.asarray(molecule.get_element_ids(), dtype=np.int64)
@@ -130,83 +131,100 @@ class ClusterLayout:
             e3 /= np.linalg.norm(e3)
             e2 = np.cross(e3, e1)
             self.frames[w] = np.stack([e1, e2, e3], axis=1)  # columns: local axes in global coordinates
-        self.rot = [atom_rotation(self.atom_ls[a], self.frames[self.water[a]].T) for a in range(len(z))]
+        # shell rotations per water (the frame rotation is Q = F^T), assembled per atom
+        per_water = [{l: sh_rotation(l, self.frames[w].T) for l in (0, 1, 2)} for w in range(len(oxy))]
+        self.rot = []
+        for a in range(len(z)):
+            mats = [per_water[self.water[a]][l] for l in self.atom_ls[a]]
+            k = sum(m.shape[0] for m in mats)
+            r = np.zeros((k, k))
+            o = 0
+            for m in mats:
+                r[o:o + m.shape[0], o:o + m.shape[0]] = m
+                o += m.shape[0]
+            self.rot.append(r)
 
     def _pairs(self):
         z, xyz = self.z, self.xyz
         n = len(z)
         dist = np.linalg.norm(xyz[:, None, :] - xyz[None, :, :], axis=2)
         self.dist = dist
-        pairs = []
-        for i in range(n):
-            pairs.append((i, i))
-        for i in range(n):
-            for j in range(n):
-                if i == j or dist[i, j] > PAIR_CUTOFF:
-                    continue
-                if z[i] == z[j] and j < i:
-                    continue
-                if z[i] == 1 and z[j] == 8:
-                    continue
-                pairs.append((i, j))
-        self.pairs = np.array(pairs, dtype=np.int64)
+        ii, jj = np.meshgrid(np.arange(n), np.arange(n), indexing='ij')
+        keep = (ii != jj) & (dist <= PAIR_CUTOFF)
+        keep &= ~((z[:, None] == z[None, :]) & (jj < ii))
+        keep &= ~((z[:, None] == 1) & (z[None, :] == 8))
+        i2, j2 = np.nonzero(keep)
+        self.pairs = np.concatenate([np.stack([np.arange(n), np.arange(n)], axis=1),
+                                     np.stack([i2, j2], axis=1)]).astype(np.int64)
+        # pairs grouped by element pair: the blocks of one group have one shape
+        self.groups = []
+        for zi, zj in ((8, 8), (8, 1), (1, 1)):
+            sel = np.where((z[self.pairs[:, 0]] == zi) & (z[self.pairs[:, 1]] == zj))[0]
+            if len(sel) == 0:
+                continue
+            a, b = self.pairs[sel, 0], self.pairs[sel, 1]
+            self.groups.append((sel, np.stack([self.atom_aos[x] for x in a]), np.stack([self.atom_aos[x] for x in b]),
+                                np.stack([self.rot[x] for x in a]), np.stack([self.rot[x] for x in b]),
+                                a == b))
 
     # ---- descriptors
-    def _env(self, i):
-        """Radial O / H neighbour densities and first moments (local frame) of atom i."""
-        d = self.dist[i]
+    def _env_all(self):
+        """Radial O / H neighbour densities and first moments (local frame) of every atom."""
+        d = self.dist
         mask = (d > 1e-8) & (d < ENV_CUTOFF)
         out = []
         for el in (8, 1):
-            sel = mask & (self.z == el)
-            out.append(np.exp(-((d[sel][:, None] - RBF_CENTERS[None, :]) / RBF_WIDTH) ** 2).sum(axis=0))
-        v = (self.xyz[mask] - self.xyz[i]) / d[mask][:, None]
-        v = v @ self.frames[self.water[i]]
-        g = np.exp(-((d[mask][:, None] - MOM_CENTERS[None, :]) / MOM_WIDTH) ** 2)
-        out.append((g[:, :, None] * v[:, None, :]).sum(axis=0).ravel())
-        return np.concatenate(out)
+            w = (mask & (self.z[None, :] == el)).astype(np.float64)
+            g = np.exp(-((d[:, :, None] - RBF_CENTERS[None, None, :]) / RBF_WIDTH) ** 2)
+            out.append((g * w[:, :, None]).sum(axis=1))
+        dsafe = np.where(mask, d, 1.0)
+        v = (self.xyz[None, :, :] - self.xyz[:, None, :]) / dsafe[:, :, None]        # [i, n, 3]
+        v = np.einsum('ink,ikl->inl', v, self.frames[self.water])                    # local frame of i
+        g = np.exp(-((d[:, :, None] - MOM_CENTERS[None, None, :]) / MOM_WIDTH) ** 2) * mask[:, :, None]
+        out.append(np.einsum('inc,inl->icl', g, v).reshape(len(self.z), -1))
+        return np.concatenate(out, axis=1)
 
     def descriptors(self):
-        n = len(self.z)
-        env = [self._env(i) for i in range(n)]
-        X = np.zeros((len(self.pairs), NFEAT), dtype=np.float32)
-        for p, (i, j) in enumerate(self.pairs):
-            zi, zj = self.z[i], self.z[j]
-            if i == j:
-                t = 0 if zi == 8 else 1
-            else:
-                t = 2 if (zi == 8 and zj == 8) else (3 if zi == 8 else 4)
-            wa, wb = self.water[i], self.water[j]
-            Fa, Fb = self.frames[wa], self.frames[wb]
-            dv = self.xyz[j] - self.xyz[i]
-            f = [np.eye(NTYPES)[t], [1.0 if wa == wb else 0.0], [self.dist[i, j], math.exp(-self.dist[i, j]),
-                                                                  1.0 / (1.0 + self.dist[i, j])],
-                 dv @ Fa, dv @ Fb, (Fa.T @ Fb).ravel(), (self.xyz[i] - self.origin[wa]) @ Fa,
-                 (self.xyz[j] - self.origin[wb]) @ Fb, env[i], env[j]]
-            X[p] = np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in f])
-        return X
+        env = self._env_all()
+        i, j = self.pairs[:, 0], self.pairs[:, 1]
+        zi, zj = self.z[i], self.z[j]
+        t = np.where(i == j, np.where(zi == 8, 0, 1), np.where((zi == 8) & (zj == 8), 2, np.where(zi == 8, 3, 4)))
+        wa, wb = self.water[i], self.water[j]
+        Fa, Fb = self.frames[wa], self.frames[wb]
+        dv = self.xyz[j] - self.xyz[i]
+        d = self.dist[i, j]
+        cols = [np.eye(NTYPES)[t], (wa == wb)[:, None].astype(np.float64),
+                np.stack([d, np.exp(-d), 1.0 / (1.0 + d)], axis=1),
+                np.einsum('pk,pkl->pl', dv, Fa), np.einsum('pk,pkl->pl', dv, Fb),
+                np.einsum('pkl,pkm->plm', Fa, Fb).reshape(len(i), 9),
+                np.einsum('pk,pkl->pl', self.xyz[i] - self.origin[wa], Fa),
+                np.einsum('pk,pkl->pl', self.xyz[j] - self.origin[wb], Fb), env[i], env[j]]
+        return np.concatenate(cols, axis=1).astype(np.float32)
 
     # ---- blocks
     def local_blocks(self, D):
         """Local-frame blocks of D (row-major, padded to NOUT) and their mask."""
         T = np.zeros((len(self.pairs), NOUT), dtype=np.float32)
         M = np.zeros((len(self.pairs), NOUT), dtype=np.float32)
-        for p, (i, j) in enumerate(self.pairs):
-            blk = self.rot[i] @ D[np.ix_(self.atom_aos[i], self.atom_aos[j])] @ self.rot[j].T
-            k = blk.size
-            T[p, :k] = blk.ravel()
-            M[p, :k] = 1.0
+        for sel, ai, aj, ri, rj, _ in self.groups:
+            blk = D[ai[:, :, None], aj[:, None, :]]
+            b = ri @ blk @ np.swapaxes(rj, 1, 2)
+            k = b.shape[1] * b.shape[2]
+            T[sel, :k] = b.reshape(len(sel), k)
+            M[sel, :k] = 1.0
         return T, M
 
     def assemble(self, B):
         """Global density from local-frame pair blocks (row-major, padded)."""
         D = np.zeros((self.nao, self.nao))
-        for p, (i, j) in enumerate(self.pairs):
-            ni, nj = len(self.atom_aos[i]), len(self.atom_aos[j])
-            blk = self.rot[i].T @ np.asarray(B[p, :ni * nj], dtype=np.float64).reshape(ni, nj) @ self.rot[j]
-            D[np.ix_(self.atom_aos[i], self.atom_aos[j])] = blk
-            if i != j:
-                D[np.ix_(self.atom_aos[j], self.atom_aos[i])] = blk.T
+        for sel, ai, aj, ri, rj, same in self.groups:
+            ni, nj = ai.shape[1], aj.shape[1]
+            b = np.asarray(B[sel, :ni * nj], dtype=np.float64).reshape(len(sel), ni, nj)
+            blk = np.swapaxes(ri, 1, 2) @ b @ rj
+            off = ~same
+            D[ai[off][:, None, :].transpose(0, 2, 1), aj[off][:, None, :]] = blk[off]
+            D[aj[off][:, :, None], ai[off][:, None, :]] = np.swapaxes(blk[off], 1, 2)
+            D[ai[same][:, :, None], aj[same][:, None, :]] = blk[same]
         return 0.5 * (D + D.T)
 
 
@@ -227,6 +245,30 @@ class LearnedGuessDriver:
         self.net = GuessMLP(data['W0'].shape[1], data['W%d' % (depth - 1)].shape[0], width, depth, device=device)
         self.net.load_state_dict(data)
         self.device = device
+
+    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None):
+        """Learned alpha density in `basis`: predicted in def2-SVP and, for any
+        other basis, carried over by the standard basis projection
+        D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis, s: def2-SVP)
+        before the idempotent projection."""
+        import torch
+        from . import _native as nat
+        from .molecularbasis import MolecularBasis
+        from .scf import SadGuessDriver
+        if basis.name.upper() == 'DEF2-SVP' and sad_density is not None:
+            return self.predict(molecule, basis, sad_density, overlap, nocc)
+        svp = MolecularBasis.read(molecule, 'def2-svp')
+        minb = MolecularBasis.read(molecule, 'ao-start-guess')
+        s_svp = nat.one_electron(0, molecule, svp, None, self.device)
+        d_svp = self.predict(molecule, svp, SadGuessDriver().compute(molecule, minb, svp, self.device), s_svp, nocc)
+        if basis.name.upper() == 'DEF2-SVP':
+            return d_svp
+        dev = self.net.dev
+        s_bs = torch.as_tensor(nat.one_electron(0, molecule, basis, svp, self.device), device=dev)
+        s_bb = torch.as_tensor(overlap, dtype=torch.float64, device=dev)
+        x = torch.linalg.solve(s_bb, s_bs)
+        d = x @ torch.as_tensor(d_svp, device=dev) @ x.T
+        return self.project(d.cpu().numpy(), overlap, nocc)
 
     def predict(self, molecule, basis, sad_density, overlap, nocc):
         import torch

@@ -183,8 +183,8 @@ class ScfRestrictedDriver:
         if guess_density is None and self.guess == 'learned':
             from .guess import LearnedGuessDriver
             t0 = time.perf_counter()
-            D_l = LearnedGuessDriver(self.guess_weights, self.device).predict(molecule, ao_basis, D_sad,
-                                                                             S.cpu().numpy(), nocc)
+            D_l = LearnedGuessDriver(self.guess_weights, self.device).predict_any(molecule, ao_basis,
+                                                                                 S.cpu().numpy(), nocc, D_sad)
             self.timings['learned_guess_s'] = time.perf_counter() - t0
             ith0 = int(-math.log10(self.dyn_threshold(1.0)))
             cands = []

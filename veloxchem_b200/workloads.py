@@ -84,17 +84,19 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
     scr.set_fp32_threshold(0.0, 0.0)
     if scf:
         runs = {}
-        for name, cut in (('fp64', 0.0), ('mixed_1e-6', 1e-6)):
+        for name, cut, guess in (('fp64_sad', 0.0, 'sad'), ('mixed_1e-6_sad', 1e-6, 'sad'),
+                                 ('fp64_learned', 0.0, 'learned'), ('mixed_1e-6_learned', 1e-6, 'learned')):
             drv = ScfRestrictedDriver()
             drv.fp32_cutoff = cut
+            drv.guess = guess
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
             runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
                           'converged': res['converged'], 'wall_s': time.perf_counter() - t0,
-                          'fock_ms_total': res['timings']['fock_ms_total'],
+                          'fock_ms_total': res['timings']['fock_ms_total'], 'guess_used': res['guess_used'],
                           'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
                                       for h in res['history']]}
-        e_ref = runs['fp64']['energy']
+        e_ref = runs['fp64_sad']['energy']
         for r in runs.values():
             r['energy_error'] = r['energy'] - e_ref
             r['time_to_1e-6_s'] = next((h[3] for k, h in enumerate(r['history'])
