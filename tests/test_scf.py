@@ -115,3 +115,24 @@ def test_sad_density_is_a_valid_guess():
     # trace(D S) = number of alpha electrons of the neutral atoms
     assert abs(np.trace(D @ S) - mol.number_of_electrons() / 2) < 1e-10
     assert np.allclose(D, D.T)
+
+
+@pytest.mark.gpu
+def test_incremental_fock_builds_reach_the_full_build_energy():
+    """Incremental builds (G of the density change, screened against max|dD|)
+    end on the energy of full builds to 1e-9 Eh; convergence is confirmed on a
+    full build, and the run does use incremental iterations."""
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200.geometry import water_cluster
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol = water_cluster((2, 2, 2), 3)
+    bas = MolecularBasis.read(mol, 'def2-svp')
+    res = {}
+    for inc in (False, True):
+        drv = ScfRestrictedDriver()
+        drv.incremental = inc
+        res[inc] = drv.compute(mol, bas)
+        assert res[inc]['converged']
+    assert abs(res[True]['scf_energy'] - res[False]['scf_energy']) < 1e-9
+    assert any(h.get('incremental') for h in res[True]['history'])
+    assert not res[True]['history'][-1].get('incremental')

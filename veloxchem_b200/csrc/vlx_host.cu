@@ -321,6 +321,39 @@ constexpr int kCoopSegment = 2;
 
 }  // namespace
 
+namespace {
+
+// Auxiliary streams over which the independent class launches of one build
+// are spread (fork from and join back into the build's stream with events),
+// so that one class's tail overlaps the next classes.
+constexpr int kFan = 4;
+struct StreamFan {
+    cudaStream_t aux[kFan] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kFan] = {};
+};
+
+int fan_create(StreamFan* f)
+{
+    for (int i = 0; i < kFan; i++) {
+        VLX_CUDA(cudaStreamCreateWithFlags(&f->aux[i], cudaStreamNonBlocking));
+        VLX_CUDA(cudaEventCreateWithFlags(&f->join[i], cudaEventDisableTiming));
+    }
+    VLX_CUDA(cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming));
+    return VLX_B200_OK;
+}
+
+void fan_destroy(StreamFan* f)
+{
+    for (int i = 0; i < kFan; i++) {
+        if (f->aux[i]) cudaStreamDestroy(f->aux[i]);
+        if (f->join[i]) cudaEventDestroy(f->join[i]);
+    }
+    if (f->fork) cudaEventDestroy(f->fork);
+}
+
+}  // namespace
+
 struct vlx_b200_screener {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -341,6 +374,7 @@ struct vlx_b200_screener {
     int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    StreamFan fan;
 };
 
 namespace {
@@ -659,6 +693,7 @@ struct LaunchCtx {
     int* counters = nullptr;
     vlx::MolDev mol{};
     const vlx::MolDev* mols = nullptr;
+    const StreamFan* fan = nullptr;  // spread the class launches over these streams (not when profiling)
 };
 
 // Enqueues all class kernels of a task set on `st`; the accumulators must be zeroed.
@@ -681,9 +716,27 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.omega2 = omega2;
     const int warps_per_block = vlx::kWarpsPerBlock;
     const int nsm = L.glob->nsm;
-    for (size_t c = 0; c < ts->classes.size(); c++) {
+    const bool fanned = L.fan && !events;
+    // launch order: most work first (the later, smaller classes fill the tails)
+    std::vector<size_t> order(ts->classes.size());
+    for (size_t c = 0; c < order.size(); c++) order[c] = c;
+    if (fanned) {
+        VLX_CUDA(cudaEventRecord(L.fan->fork, st));
+        for (int i = 0; i < kFan; i++) VLX_CUDA(cudaStreamWaitEvent(L.fan->aux[i], L.fan->fork, 0));
+        std::vector<double> cost(order.size());
+        for (size_t c = 0; c < order.size(); c++) {
+            const ClassTasks& ct = ts->classes[c];
+            const int pf = ct.compiled >= 0 ? vlx::kQuartetClasses[ct.compiled].prim_flops : L.glob->coop_prim_flops[ct.coop];
+            const int qf = ct.compiled >= 0 ? vlx::kQuartetClasses[ct.compiled].post_flops : L.glob->coop_post_flops[ct.coop];
+            cost[c] = (double)ct.prim_quartets * pf + (double)ct.quartets * qf;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
+    }
+    int slot = 0;
+    for (size_t c : order) {
         ClassTasks& ct = ts->classes[c];
         if (ct.items.empty() && ct.items32.empty()) continue;
+        const cudaStream_t cs = fanned ? L.fan->aux[slot++ % kFan] : st;
         a.items = ts->d_items + ct.offset;
         a.nitems = (int)ct.items.size();
         a.counter = L.counters + c;
@@ -693,7 +746,7 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
             const auto& e = vlx::kQuartetClasses[ct.compiled];
             const int occ = std::max(1, e.occupancy(mode));
             if (!ct.items.empty()) {
-                e.launch(mode, a, std::max(1, std::min(want, occ * nsm)), st);
+                e.launch(mode, a, std::max(1, std::min(want, occ * nsm)), cs);
                 if (launches) (*launches)++;
             }
             if (!ct.items32.empty()) {
@@ -702,7 +755,7 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
                 a32.nitems = (int)ct.items32.size();
                 a32.counter = L.counters + ts->classes.size() + c;
                 const int want32 = (int)((ct.items32.size() + warps_per_block - 1) / warps_per_block);
-                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * nsm)), st);
+                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * nsm)), cs);
                 if (launches) (*launches)++;
             }
         } else {
@@ -717,12 +770,18 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
                 const int wpb = vlx::coop_warps_per_block(cc, f != 0);
                 const int cap = vlx::coop_blocks_per_sm(cc, f != 0) * nsm;
                 const int grid = std::max(1, std::min((int)((its.size() + wpb - 1) / wpb), cap));
-                VLX_CUDA(vlx::launch_coop_quartet(f ? (mode | vlx::MODE_F32) : mode, ac, cc, grid, st));
+                VLX_CUDA(vlx::launch_coop_quartet(f ? (mode | vlx::MODE_F32) : mode, ac, cc, grid, cs));
                 if (launches) (*launches)++;
             }
         }
         VLX_CUDA(cudaGetLastError());
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].second, st));
+    }
+    if (fanned) {
+        for (int i = 0; i < kFan; i++) {
+            VLX_CUDA(cudaEventRecord(L.fan->join[i], L.fan->aux[i]));
+            VLX_CUDA(cudaStreamWaitEvent(st, L.fan->join[i], 0));
+        }
     }
     return VLX_B200_OK;
 }
@@ -739,6 +798,7 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     L.mol.F = dAcc;
     L.mol.nao = s->nao;
     for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
+    L.fan = &s->fan;
     return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, st, launches, events);
 }
 
@@ -890,6 +950,8 @@ int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, co
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) ||
         cudaEventCreate(&s->ev0) || cudaEventCreate(&s->ev1))
         return cleanup(fail(VLX_B200_ERR_CUDA, "screener_create: stream / event creation failed"));
+    rc = fan_create(&s->fan);
+    if (rc) return cleanup(rc);
     // shells and the AO map (MolecularBasis.cpp:468-490)
     size_t off = 0;
     s->shells.resize(nshells);
@@ -989,6 +1051,7 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    fan_destroy(&s->fan);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return VLX_B200_OK;
@@ -1506,6 +1569,7 @@ struct vlx_b200_batch {
     int key_sym = -1, key_ith = -1;
     double key_cj = 0.0, key_ck = 0.0, key_om2 = -1.0;
     const double* mols_D = nullptr;  // D of the uploaded per-molecule records
+    StreamFan fan;
     long long launches = 0;          // kernel launches of one build
 };
 
@@ -1599,6 +1663,7 @@ int batch_enqueue(vlx_b200_batch* b, TaskSet* ts, bool known, int symmetric, dou
         L.glob = b->glob;
         L.counters = b->d_counters;
         L.mols = b->d_mols;
+        L.fan = &b->fan;
         const int rc = enqueue_ctx(L, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, nullptr, cj, ck,
                                    omega2, st, launches);
         if (rc) return rc;
@@ -1658,6 +1723,10 @@ int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screen
     if (blocks.size() > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: more than 65535 pair blocks");
     VLX_CUDA(cudaSetDevice(b->device));
     VLX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    {
+        const int rc = fan_create(&b->fan);
+        if (rc) return rc;
+    }
     VLX_CUDA(cudaMalloc(&b->d_blocks, std::max<size_t>(1, blocks.size()) * sizeof(PairBlockDev)));
     if (!blocks.empty())
         VLX_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), blocks.size() * sizeof(PairBlockDev), cudaMemcpyHostToDevice));
@@ -1684,6 +1753,7 @@ int vlx_b200_batch_destroy(vlx_b200_batch* b)
     cudaFree(b->d_nao);
     cudaFree(b->d_acc);
     if (b->d_counters) cudaFree(b->d_counters);
+    fan_destroy(&b->fan);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return VLX_B200_OK;

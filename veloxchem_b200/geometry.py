@@ -81,6 +81,7 @@ def batch_clusters(count=256, nmax=16, seed=7, lattice=(3, 3, 2)):
 # Named workloads (lattice, seed).
 CLUSTERS = {
     'h2o4': ((2, 2, 1), 1),
+    'h2o8': ((2, 2, 2), 1),     # small profiling case
     'h2o32': ((4, 4, 2), 1),
     'h2o64': ((4, 4, 4), 1),
 }

@@ -230,6 +230,17 @@ class ClusterLayout:
 
 # ------------------------------------------------------------ the guess driver
 
+_DRIVERS = {}
+
+
+def learned_guess_driver(weights=None, device=0):
+    """The driver of a weights file on a device, loaded once per process."""
+    key = (str(WEIGHTS if weights is None else weights), int(device))
+    if key not in _DRIVERS:
+        _DRIVERS[key] = LearnedGuessDriver(weights, device)
+    return _DRIVERS[key]
+
+
 class LearnedGuessDriver:
     """Predicts the alpha density of a water cluster in def2-SVP from the
     trained network (BF16 inference on the GPU) on top of SAD."""
@@ -246,7 +257,7 @@ class LearnedGuessDriver:
         self.net.load_state_dict(data)
         self.device = device
 
-    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None):
+    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None, ortho=None):
         """Learned alpha density in `basis`: predicted in def2-SVP and, for any
         other basis, carried over by the standard basis projection
         D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis, s: def2-SVP)
@@ -256,7 +267,7 @@ class LearnedGuessDriver:
         from .molecularbasis import MolecularBasis
         from .scf import SadGuessDriver
         if basis.name.upper() == 'DEF2-SVP' and sad_density is not None:
-            return self.predict(molecule, basis, sad_density, overlap, nocc)
+            return self.predict(molecule, basis, sad_density, overlap, nocc, ortho)
         svp = MolecularBasis.read(molecule, 'def2-svp')
         minb = MolecularBasis.read(molecule, 'ao-start-guess')
         s_svp = nat.one_electron(0, molecule, svp, None, self.device)
@@ -268,30 +279,33 @@ class LearnedGuessDriver:
         s_bb = torch.as_tensor(overlap, dtype=torch.float64, device=dev)
         x = torch.linalg.solve(s_bb, s_bs)
         d = x @ torch.as_tensor(d_svp, device=dev) @ x.T
-        return self.project(d.cpu().numpy(), overlap, nocc)
+        return self.project(d.cpu().numpy(), overlap, nocc, ortho)
 
-    def predict(self, molecule, basis, sad_density, overlap, nocc):
+    def predict(self, molecule, basis, sad_density, overlap, nocc, ortho=None):
         import torch
         lay = ClusterLayout(molecule, basis)
         X = (lay.descriptors() - self.mu) / self.sd
         y = self.net.predict_bf16(torch.tensor(X, device=self.net.dev)).cpu().numpy()
         Tsad, _ = lay.local_blocks(sad_density)
         D = lay.assemble(Tsad + y / self.scale)
-        return self.project(D, overlap, nocc)
+        return self.project(D, overlap, nocc, ortho)
 
-    def project(self, D, overlap, nocc):
+    def project(self, D, overlap, nocc, ortho=None):
         """Nearest idempotent density with nocc electrons: the nocc natural
-        orbitals of largest occupation of D (eigenvectors of S^1/2 D S^1/2),
-        so that the first-iteration energy is variational."""
+        orbitals of largest occupation of D, i.e. the leading eigenvectors of
+        X^T S D S X for an orthogonaliser X of the AO basis (X^T S X = 1;
+        the SCF driver's canonical X when given, else S^-1/2), so that the
+        first-iteration energy is variational."""
         import torch
         dev = self.net.dev
         S = torch.as_tensor(overlap, dtype=torch.float64, device=dev)
-        w, u = torch.linalg.eigh(S)
-        keep = w > 1.0e-6
-        u, w = u[:, keep], w[keep]
-        sh = (u * torch.sqrt(w)) @ u.T
-        sih = (u / torch.sqrt(w)) @ u.T
+        if ortho is None:
+            w, u = torch.linalg.eigh(S)
+            keep = w > 1.0e-6
+            ortho = u[:, keep] / torch.sqrt(w[keep])
+        X = torch.as_tensor(ortho, dtype=torch.float64, device=dev)
         Dt = torch.as_tensor(D, dtype=torch.float64, device=dev)
-        n, v = torch.linalg.eigh(sh @ Dt @ sh)
-        C = sih @ v[:, -nocc:]
+        M = X.T @ S @ Dt @ S @ X
+        n, v = torch.linalg.eigh(0.5 * (M + M.T))
+        C = X @ v[:, -nocc:]
         return (C @ C.T).cpu().numpy()

@@ -22,7 +22,10 @@ scfrestdriver.py) for the parts a restricted HF energy needs:
   commutator (the reference uses C2-DIIS, c2diis.py), MOs from X^T F X and
   D = C_occ C_occ^T (scfrestdriver.py:214-269);
 * convergence when the electronic gradient is below ``conv_thresh``
-  (default 1e-6, scfdriver.py:151).
+  (default 1e-6, scfdriver.py:151);
+* incremental Fock builds with density-difference screening (the reference
+  SCF builds from the full density each iteration); convergence is always
+  confirmed on a full FP64 build.
 
 Linear algebra runs in FP64 with torch on the same GPU; the Fock build is the
 native library's.
@@ -118,6 +121,13 @@ class ScfRestrictedDriver:
         # final iterations are FP64, so the converged energy is the FP64 one
         self.fp32_cutoff = 0.0
         self.fp32_until_grad = 1.0e-4
+        # incremental Fock builds: F_n = F_(n-1) + G(D_n - D_(n-1)) with the
+        # screening threshold tightened by max|D_n - D_(n-1)| (a quartet is
+        # dropped when its Schwarz bound times max|dD| is below the dynamic
+        # threshold); a full build every rebuild_every iterations, whenever
+        # the dynamic threshold changes, and to confirm convergence
+        self.incremental = True
+        self.rebuild_every = 10
         self.history = []
         self.timings = {}
 
@@ -181,10 +191,10 @@ class ScfRestrictedDriver:
         first = None  # (F2e) of the first iteration, when the guess selection already built it
         self.guess_used = self.guess if guess_density is None else 'given'
         if guess_density is None and self.guess == 'learned':
-            from .guess import LearnedGuessDriver
+            from .guess import learned_guess_driver
             t0 = time.perf_counter()
-            D_l = LearnedGuessDriver(self.guess_weights, self.device).predict_any(molecule, ao_basis,
-                                                                                 S.cpu().numpy(), nocc, D_sad)
+            D_l = learned_guess_driver(self.guess_weights, self.device).predict_any(molecule, ao_basis,
+                                                                                   S.cpu().numpy(), nocc, D_sad, X)
             self.timings['learned_guess_s'] = time.perf_counter() - t0
             ith0 = int(-math.log10(self.dyn_threshold(1.0)))
             cands = []
@@ -201,35 +211,64 @@ class ScfRestrictedDriver:
         self.history = []
         converged = False
         fock_ms = 0.0
+        D_prev, F2e_prev, ith_prev, since_full = None, None, -1, 0
+        G = torch.empty_like(D)
+
+        def evaluate(F2e):
+            e_ee = torch.sum(D * F2e)
+            e_one = 2.0 * torch.sum(D * H)
+            F = F2e + H
+            fds = F @ D @ S
+            err = X.T @ (fds - fds.T) @ X
+            return float(e_ee + e_one) + e_nuc, F, err, 2.0 * float(torch.linalg.norm(err))
+
         for it in range(1, self.max_iter + 1):
             ith = int(-math.log10(self.dyn_threshold(e_grad)))
             D = 0.5 * (D + D.T).contiguous()
             mixed = self.fp32_cutoff > 0.0 and e_grad > self.fp32_until_grad
-            if mixed:
-                screener.set_fp32_threshold(self.fp32_cutoff, float(torch.max(torch.abs(D))))
-            else:
-                screener.set_fp32_threshold(0.0, 0.0)
+            inc = (self.incremental and first is None and D_prev is not None and ith == ith_prev
+                   and since_full + 1 < self.rebuild_every)
             t0 = time.perf_counter()
             if first is not None:
                 F2e.copy_(first)
                 first = None
+                ith_used = ith
+            elif inc:
+                dD = (D - D_prev).contiguous()
+                m = float(torch.max(torch.abs(dD)))
+                ith_used = max(0, ith + math.floor(math.log10(m))) if 0.0 < m < 1.0 else ith
+                screener.set_fp32_threshold(self.fp32_cutoff if mixed else 0.0, m)
+                build(dD, G, ith_used)
+                F2e.copy_(F2e_prev)
+                F2e.add_(G)
             else:
+                screener.set_fp32_threshold(self.fp32_cutoff if mixed else 0.0, float(torch.max(torch.abs(D))))
                 build(D, F2e, ith)
+                ith_used = ith
             torch.cuda.synchronize(dev)
             fock_ms += 1e3 * (time.perf_counter() - t0)
-            e_ee = torch.sum(D * F2e)
-            e_one = 2.0 * torch.sum(D * H)
-            F = F2e + H
-            energy = float(e_ee + e_one) + e_nuc
-            fds = F @ D @ S
-            err = X.T @ (fds - fds.T) @ X
-            e_grad = 2.0 * float(torch.linalg.norm(err))
+            since_full = since_full + 1 if inc else 0
+            energy, F, err, e_grad = evaluate(F2e)
             self.history.append({'iteration': it, 'energy': energy, 'delta_e': energy - e_old, 'e_grad': e_grad,
-                                 'ithreshold': ith, 'mixed': mixed, 'time_s': time.perf_counter() - t_start})
+                                 'ithreshold': ith_used, 'mixed': mixed, 'incremental': inc,
+                                 'time_s': time.perf_counter() - t_start})
             e_old = energy
+            if e_grad < self.conv_thresh and inc:
+                # confirm on a full FP64 build of the same density
+                t0 = time.perf_counter()
+                screener.set_fp32_threshold(0.0, 0.0)
+                build(D, F2e, ith)
+                torch.cuda.synchronize(dev)
+                fock_ms += 1e3 * (time.perf_counter() - t0)
+                since_full = 0
+                energy, F, err, e_grad = evaluate(F2e)
+                self.history.append({'iteration': it, 'energy': energy, 'delta_e': energy - e_old, 'e_grad': e_grad,
+                                     'ithreshold': ith, 'mixed': False, 'incremental': False, 'check': True,
+                                     'time_s': time.perf_counter() - t_start})
             if e_grad < self.conv_thresh:
                 converged = True
                 break
+            D_prev, F2e_prev, ith_prev = D, F2e.clone(), ith
             focks.append(F)
             errs.append(err)
             if len(focks) > self.max_err_vecs:
@@ -243,7 +282,8 @@ class ScfRestrictedDriver:
         self.timings['fock_ms_total'] = fock_ms
         self.timings['total_s'] = time.perf_counter() - t_start
         e, c = torch.linalg.eigh(X.T @ F @ X)
-        return {'scf_energy': energy, 'converged': converged, 'iterations': len(self.history),
+        return {'scf_energy': energy, 'converged': converged,
+                'iterations': sum(1 for h in self.history if not h.get('check')),
                 'e_grad': e_grad, 'nuclear_repulsion': e_nuc, 'D_alpha': D.cpu().numpy(),
                 'C_alpha': (X @ c).cpu().numpy(), 'E_alpha': e.cpu().numpy(), 'F_alpha': F.cpu().numpy(),
                 'history': self.history, 'timings': dict(self.timings), 'screener': screener,

@@ -144,7 +144,7 @@ def evaluate(weights, count, nwaters, seed, log=print):
             conv_it = next((h['iteration'] for h in r['history'] if h['e_grad'] < 1e-6), None)
             row[name] = {'iterations_to_grad_1e-6': conv_it, 'converged': r['converged'], 'wall_s': r['wall_s'],
                          'iters_to_1e-6': it, 'time_to_1e-6_s': ts, 'energy_error': r['scf_energy'] - e_ref,
-                         'guess_used': r.get('guess_used')}
+                         'guess_used': r.get('guess_used'), 'learned_guess_s': r['timings'].get('learned_guess_s')}
         row['learned']['guess_energies'] = lrn['timings'].get('guess_energies')
         rows.append(row)
         log('eval %d: SAD %s it %.2f s | learned (%s) %s it %.2f s' %

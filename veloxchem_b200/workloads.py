@@ -84,11 +84,16 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
     scr.set_fp32_threshold(0.0, 0.0)
     if scf:
         runs = {}
-        for name, cut, guess in (('fp64_sad', 0.0, 'sad'), ('mixed_1e-6_sad', 1e-6, 'sad'),
-                                 ('fp64_learned', 0.0, 'learned'), ('mixed_1e-6_learned', 1e-6, 'learned')):
+        # plain: FP64 builds from the full density every iteration, SAD guess
+        for name, cut, guess, inc in (('plain_fp64_sad', 0.0, 'sad', False),
+                                      ('fp64_sad_incremental', 0.0, 'sad', True),
+                                      ('mixed_1e-6_sad', 1e-6, 'sad', False),
+                                      ('fp64_learned', 0.0, 'learned', False),
+                                      ('mixed_learned_incremental', 1e-6, 'learned', True)):
             drv = ScfRestrictedDriver()
             drv.fp32_cutoff = cut
             drv.guess = guess
+            drv.incremental = inc
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
             runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
@@ -96,7 +101,7 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
                           'fock_ms_total': res['timings']['fock_ms_total'], 'guess_used': res['guess_used'],
                           'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
                                       for h in res['history']]}
-        e_ref = runs['fp64_sad']['energy']
+        e_ref = runs['plain_fp64_sad']['energy']
         for r in runs.values():
             r['energy_error'] = r['energy'] - e_ref
             r['time_to_1e-6_s'] = next((h[3] for k, h in enumerate(r['history'])
@@ -169,26 +174,54 @@ def c2scf():
     from .scf import ScfRestrictedDriver
     mol, bas = _cluster('h2o32', 'def2-svp')
     runs = {}
-    for name, cut in (('warmup', 0.0), ('fp64', 0.0), ('mixed_1e-6', 1e-6)):
+    for name, cut, inc in (('warmup', 0.0, False), ('plain_fp64', 0.0, False), ('mixed_1e-6', 1e-6, False),
+                           ('fp64_incremental', 0.0, True), ('mixed_incremental', 1e-6, True)):
         drv = ScfRestrictedDriver()
         drv.fp32_cutoff = cut
+        drv.incremental = inc
         t0 = time.perf_counter()
         res = drv.compute(mol, bas)
         if name == 'warmup':
             continue
         runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
                       'wall_s': time.perf_counter() - t0, 'fock_ms_total': res['timings']['fock_ms_total']}
-    runs['energy_error_mixed'] = runs['mixed_1e-6']['energy'] - runs['fp64']['energy']
+    for k in ('mixed_1e-6', 'fp64_incremental', 'mixed_incremental'):
+        runs[k]['energy_error'] = runs[k]['energy'] - runs['plain_fp64']['energy']
     return {'workload': '(H2O)32 / def2-SVP RHF from SAD, gradient < 1e-6', **runs}
+
+
+def build(cluster, basis, repeat=1, fp32_cutoff=0.0):
+    """Screener + `repeat` plain builds of a named cluster (the command the
+    profiles under profiles/ are taken on)."""
+    from . import T4CScreener
+    from .geometry import random_density
+    torch = _torch()
+    mol, bas = _cluster(cluster, basis)
+    scr = T4CScreener()
+    scr.partition(bas, mol, 'eri')
+    d = torch.from_numpy(random_density(scr.nao, 5 * mol.number_of_atoms() // 3, 1)).cuda()
+    if fp32_cutoff > 0:
+        scr.set_fp32_threshold(fp32_cutoff, float(d.abs().max()))
+    f = torch.empty_like(d)
+    ms = [_build_ms(scr, d, f, reps=0) for _ in range(repeat)]
+    return {'workload': '%s / %s, 2J-K, ithreshold 12' % (cluster, basis), 'nao': scr.nao, 'build_ms': ms,
+            'fp32_cutoff': fp32_cutoff}
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument('which', choices=['c3', 'c4', 'c2scf'])
+    ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build'])
     ap.add_argument('--out', default=None)
     ap.add_argument('--no-scf', action='store_true')
+    ap.add_argument('--cluster', default='h2o64')
+    ap.add_argument('--basis', default='def2-tzvp')
+    ap.add_argument('--repeat', type=int, default=1)
+    ap.add_argument('--fp32-cutoff', type=float, default=0.0)
     a = ap.parse_args(argv)
-    res = c3(scf=not a.no_scf) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf())
+    if a.which == 'build':
+        res = build(a.cluster, a.basis, a.repeat, a.fp32_cutoff)
+    else:
+        res = c3(scf=not a.no_scf) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf())
     text = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, 'w') as fh:
