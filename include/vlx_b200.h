@@ -84,6 +84,13 @@ int vlx_b200_screener_pair_info(const vlx_b200_screener* screener, int* info, do
  * GPU work item is 256 / factor, at least 32. */
 int vlx_b200_set_block_size_factor(vlx_b200_screener* screener, int factor);
 
+/* Work lists of later builds are made for max(ithreshold, ithreshold_base)
+ * and the quartets above a build's own ithreshold are skipped at run time, so
+ * that builds at several thresholds (the SCF's dynamic threshold, the tighter
+ * thresholds of incremental builds) share one list.  -1 (default): lists are
+ * made for each threshold.  No counterpart in the reference. */
+int vlx_b200_set_work_threshold(vlx_b200_screener* screener, int ithreshold_base);
+
 /* One Fock matrix.  density / fock_out: host nao x nao.  symmetric != 0 for a
  * symmetric density (reference mat_t::symmetric), else general.
  * label: "2jk", "2jkx", "j", "k", "kx", and "j_rs", "k_rs", "kx_rs", which
@@ -271,6 +278,24 @@ int vlx_b200_adam_step(float* params, const float* grads, float* m, float* v, lo
 
 /* FP32 -> BF16 (round to nearest even). */
 int vlx_b200_to_bf16(const float* x, void* y_bf16, long long n, void* stream);
+
+/* ---- autotuning (no counterpart in the reference, whose block-size factor
+ * is one global knob: CFockDriver::set_block_size_factor,
+ * src/t4c_func/FockDriver.cpp:356-404).  Times every quartet class of a
+ * 2J-K build of d_density at `ithreshold` under several ket-run lengths per
+ * work item and keeps the fastest per class for the screener's later builds
+ * (all thresholds); synchronises `stream`.  Results are numerically the same
+ * builds (only the order of the FP64 atomic additions changes). */
+typedef struct {
+    int la, lb, lc, ld;
+    int table_driven;   /* 1: warp-cooperative kernel */
+    int segment;        /* chosen ket pairs per work item */
+    double best_ms;     /* device time of the class with the chosen length */
+    double default_ms;  /* ... with the default length */
+} vlx_b200_tune_result;
+
+int vlx_b200_autotune(vlx_b200_screener* screener, const double* d_density, int ithreshold, void* stream,
+                      int max_classes, vlx_b200_tune_result* out, int* nclasses);
 
 #ifdef __cplusplus
 }

@@ -272,3 +272,34 @@ def test_mixed_precision_scf_energy():
     res = drv.compute(mol, bas)
     assert res['converged'] and any(h['mixed'] for h in res['history'])
     assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
+
+
+def test_autotune_keeps_the_result():
+    """Per-class work-item lengths chosen by timing change only the order of
+    the FP64 additions: the build after tuning equals the one before (1e-12)."""
+    import torch
+    from veloxchem_b200 import _native as nat
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    d = torch.from_numpy(g['density']).cuda()
+    before = _fock(s, g['density'], '2jk', 1.0, 12)
+    res = nat.autotune(s, d.data_ptr(), 12)
+    torch.cuda.synchronize()
+    assert res and all(r['segment'] > 0 and r['best_ms'] <= r['default_ms'] for r in res)
+    after = _fock(s, g['density'], '2jk', 1.0, 12)
+    assert np.max(np.abs(after - before)) < 1e-12
+    assert np.max(np.abs(after - g['f2jk'])) < TOL
+
+
+def test_shared_work_list_filters_thresholds_at_run_time():
+    """One work list built for ithreshold 15 serves builds at looser
+    thresholds: the quartets above each build's threshold are skipped in the
+    kernels, and every result equals the oracle at that threshold."""
+    from oracle.oracle import PortOracle
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    s.set_work_threshold(15)
+    ref = PortOracle(mol, bas)
+    for ith in (4, 8, 12, 15):
+        f = _fock(s, g['density'], '2jk', 1.0, ith)
+        assert np.max(np.abs(f - ref.fock(g['density'], '2jk', 1.0, ith))) < TOL, ith

@@ -59,6 +59,8 @@ SIGNATURES = {
     'vlx_b200_adam_step': (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_float, ctypes.c_float,
                                           ctypes.c_float, ctypes.c_float, ctypes.c_int, _vp]),
     'vlx_b200_to_bf16': (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp]),
+    'vlx_b200_set_work_threshold': (ctypes.c_int, [_vp, ctypes.c_int]),
+    'vlx_b200_autotune': (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _ip]),
     'vlx_b200_batch_create': (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int]),
     'vlx_b200_batch_destroy': (ctypes.c_int, [_vp]),
     'vlx_b200_batch_offsets': (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
@@ -75,6 +77,25 @@ class ClassProfile(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [('la', ctypes.c_int), ('lb', ctypes.c_int), ('lc', ctypes.c_int), ('ld', ctypes.c_int),
+                ('table_driven', ctypes.c_int), ('segment', ctypes.c_int), ('best_ms', ctypes.c_double),
+                ('default_ms', ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def autotune(screener, d_density_ptr, ithreshold=12, stream_ptr=None, max_classes=256):
+    """Per-class work-item lengths for the screener's later builds; returns the choices."""
+    arr = (TuneResult * max_classes)()
+    n = ctypes.c_int(0)
+    check(lib().vlx_b200_autotune(screener.handle, ctypes.c_void_p(d_density_ptr), int(ithreshold),
+                                  ctypes.c_void_p(stream_ptr) if stream_ptr else None, max_classes,
+                                  ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(n)), 'autotune')
+    return [arr[i].as_dict() for i in range(n.value)]
 
 
 def fp64_peak(device=0):

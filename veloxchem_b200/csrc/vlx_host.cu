@@ -302,13 +302,13 @@ struct ClassTasks {
     int coop = -1;      // index into DeviceGlobals::coop
     int la = 0, lb = 0, lc = 0, ld = 0;
     std::vector<WorkItem> items;    // FP64 quartets
-    std::vector<WorkItem> items32;  // FP32 quartets (mixed precision)
+    std::vector<WorkItem> items32;  // unused (the FP32 part of an item is selected at run time)
     size_t offset = 0, offset32 = 0;
     long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0, fp32_quartets = 0;
 };
 
 struct TaskSet {
-    int ith = 0, rank = 0, nodes = 1, seg = 0, ith32 = -1;
+    int ith = 0, rank = 0, nodes = 1, seg = 0, tune_gen = 0;  // ith: the threshold the items were built for
     std::vector<ClassTasks> classes;
     WorkItem* d_items = nullptr;
     long long quartets = 0, prim_quartets = 0;
@@ -318,39 +318,6 @@ int pair_key(int la, int lb) { return (la + lb) * 16 + lb; }
 
 // ket pairs per work item of a warp-cooperative class
 constexpr int kCoopSegment = 2;
-
-}  // namespace
-
-namespace {
-
-// Auxiliary streams over which the independent class launches of one build
-// are spread (fork from and join back into the build's stream with events),
-// so that one class's tail overlaps the next classes.
-constexpr int kFan = 4;
-struct StreamFan {
-    cudaStream_t aux[kFan] = {};
-    cudaEvent_t fork = nullptr;
-    cudaEvent_t join[kFan] = {};
-};
-
-int fan_create(StreamFan* f)
-{
-    for (int i = 0; i < kFan; i++) {
-        VLX_CUDA(cudaStreamCreateWithFlags(&f->aux[i], cudaStreamNonBlocking));
-        VLX_CUDA(cudaEventCreateWithFlags(&f->join[i], cudaEventDisableTiming));
-    }
-    VLX_CUDA(cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming));
-    return VLX_B200_OK;
-}
-
-void fan_destroy(StreamFan* f)
-{
-    for (int i = 0; i < kFan; i++) {
-        if (f->aux[i]) cudaStreamDestroy(f->aux[i]);
-        if (f->join[i]) cudaEventDestroy(f->join[i]);
-    }
-    if (f->fork) cudaEventDestroy(f->fork);
-}
 
 }  // namespace
 
@@ -371,10 +338,14 @@ struct vlx_b200_screener {
     int* d_counters = nullptr;
     int ncounters = 0;
     int seg = 256;
+    // autotuned ket-run length per quartet class (key la | lb << 4 | lc << 8 | ld << 12)
+    std::map<int, int> class_seg;
+    int tune_gen = 0;                          // bumped whenever class_seg changes (task-set cache key)
+    int seg_try_compiled = 0, seg_try_coop = 0;  // candidate lengths while tuning (0: off)
     int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
+    int ith_base = -1;  // work lists are built for max(ithreshold, ith_base) and filtered at run time
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    StreamFan fan;
 };
 
 namespace {
@@ -391,7 +362,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         const size_t n = sorted ? pb.sorted.size() : pb.pairs.size();
         npairs[b] = (int)n;
         const size_t k = (size_t)pb.ka * pb.kb;
-        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + 3 * n * sizeof(int);
+        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + (4 * n + 17) * sizeof(int);
         bytes = (bytes + 255) & ~size_t(255);
         offs[b + 1] = offs[b] + bytes;
     }
@@ -407,7 +378,11 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         double* ab = prim + 9 * (size_t)kp * n;
         int* ao = reinterpret_cast<int*>(ab + 3 * n);
         int* nuse = ao + 2 * n;
+        int* bins = nuse + n;     // Schwarz bin per pair (sorted order; 0 before screening)
+        int* bin_off = bins + n;  // first pair of bin >= b (17 entries)
+        for (int k = 0; k <= 16; k++) bin_off[k] = sorted ? pb.bin_off[k] : 0;
         for (size_t i = 0; i < n; i++) {
+            bins[i] = sorted ? pb.bin[pb.sorted[i]] : 0;
             const int ref = sorted ? pb.sorted[i] : (int)i;
             const Shell& A = s->shells[pb.pairs[ref].first];
             const Shell& B = s->shells[pb.pairs[ref].second];
@@ -466,6 +441,8 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         d.ab = d.prim + 9 * (size_t)kp * n;
         d.ao = reinterpret_cast<const int*>(d.ab + 3 * n);
         d.nuse = d.ao + 2 * n;
+        d.bin = d.nuse + n;
+        d.bin_off = d.bin + n;
         d.npairs = (int)n;
         d.kprim = kp;
         d.la = pb.la;
@@ -529,10 +506,11 @@ int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
     return VLX_B200_OK;
 }
 
-int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** out)
+int build_tasks(vlx_b200_screener* s, int ith_req, int rank, int nodes, TaskSet** out)
 {
+    const int ith = std::max(ith_req, s->ith_base);
     for (auto& t : s->tasksets)
-        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg && t.ith32 == s->ith32) {
+        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg && t.tune_gen == s->tune_gen) {
             *out = &t;
             return VLX_B200_OK;
         }
@@ -541,7 +519,7 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
     ts.rank = rank;
     ts.nodes = nodes;
     ts.seg = s->seg;
-    ts.ith32 = s->ith32;
+    ts.tune_gen = s->tune_gen;
     std::map<int, int> cls_index;  // key -> position in ts.classes
     long long g = 0;
     const size_t nb = s->blocks.size();
@@ -581,33 +559,22 @@ int build_tasks(vlx_b200_screener* s, int ith, int rank, int nodes, TaskSet** ou
                 const int kbeg = diag ? x : 0;
                 // a compiled-class item feeds 32 lanes per step; a cooperative-class
                 // item is walked one quartet at a time by one warp, so it stays short
-                const int seg = (ct.coop >= 0) ? kCoopSegment : s->seg;
+                int seg = (ct.coop >= 0) ? kCoopSegment : s->seg;
+                if (s->seg_try_compiled > 0) {
+                    seg = (ct.coop >= 0) ? s->seg_try_coop : s->seg_try_compiled;
+                } else {
+                    const auto tuned = s->class_seg.find(ct.la | (ct.lb << 4) | (ct.lc << 8) | (ct.ld << 12));
+                    if (tuned != s->class_seg.end()) seg = tuned->second;
+                }
                 for (int k0 = kbeg; k0 < kend; k0 += seg) {
                     const int k1 = std::min(kend, k0 + seg);
                     if ((g++ % nodes) != rank) continue;
-                    // mixed precision: kets are bin-sorted, so the quartets whose bound
-                    // 10^-(bin_bra + bin_ket) times max|D| is below the FP32 cutoff
-                    // are the tail [k_mid, k1) of the run
-                    int k_mid = k1;
-                    if (s->ith32 >= 0) {
-                        const int b32 = s->ith32 - bx;
-                        const int kb32 = (b32 <= 0) ? 0 : Pk.bin_off[std::min(b32, 16)];
-                        k_mid = std::min(k1, std::max(k0, kb32));
-                    }
                     WorkItem w;
                     w.blocks = (int)bra | ((int)ket << 16);
                     w.bra = x;
-                    if (k_mid > k0) {
-                        w.kbeg = k0;
-                        w.kend = k_mid;
-                        ct.items.push_back(w);
-                    }
-                    if (k1 > k_mid) {
-                        w.kbeg = k_mid;
-                        w.kend = k1;
-                        ct.items32.push_back(w);
-                        ct.fp32_quartets += k1 - k_mid;
-                    }
+                    w.kbeg = k0;
+                    w.kend = k1;
+                    ct.items.push_back(w);
                     const long long evaluated =
                         (long long)Pb.nuse[x] * (Pk.nuse_prefix[k1] - Pk.nuse_prefix[k0]);
                     ts.quartets += k1 - k0;
@@ -693,12 +660,15 @@ struct LaunchCtx {
     int* counters = nullptr;
     vlx::MolDev mol{};
     const vlx::MolDev* mols = nullptr;
-    const StreamFan* fan = nullptr;  // spread the class launches over these streams (not when profiling)
 };
 
-// Enqueues all class kernels of a task set on `st`; the accumulators must be zeroed.
+// Enqueues all class kernels of a task set on `st`; the accumulators must be
+// zeroed.  Quartets with bin sum <= ith (<= the threshold the task set was
+// built for) are evaluated; with ith32 >= 0 every class is launched twice
+// over the same work items, the FP64 launch taking the kets below the FP32
+// boundary of each item and the FP32 launch the rest.
 int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double cj, double ck, double omega2,
-                cudaStream_t st, long long* launches,
+                int ith, int ith32, cudaStream_t st, long long* launches,
                 std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
 {
     if (ts->classes.empty()) return VLX_B200_OK;
@@ -714,80 +684,42 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.cj = cj;
     a.ck = ck;
     a.omega2 = omega2;
+    a.ith = std::min(ith, ts->ith);
+    a.ith32 = ith32;
     const int warps_per_block = vlx::kWarpsPerBlock;
     const int nsm = L.glob->nsm;
-    const bool fanned = L.fan && !events;
-    // launch order: most work first (the later, smaller classes fill the tails)
-    std::vector<size_t> order(ts->classes.size());
-    for (size_t c = 0; c < order.size(); c++) order[c] = c;
-    if (fanned) {
-        VLX_CUDA(cudaEventRecord(L.fan->fork, st));
-        for (int i = 0; i < kFan; i++) VLX_CUDA(cudaStreamWaitEvent(L.fan->aux[i], L.fan->fork, 0));
-        std::vector<double> cost(order.size());
-        for (size_t c = 0; c < order.size(); c++) {
-            const ClassTasks& ct = ts->classes[c];
-            const int pf = ct.compiled >= 0 ? vlx::kQuartetClasses[ct.compiled].prim_flops : L.glob->coop_prim_flops[ct.coop];
-            const int qf = ct.compiled >= 0 ? vlx::kQuartetClasses[ct.compiled].post_flops : L.glob->coop_post_flops[ct.coop];
-            cost[c] = (double)ct.prim_quartets * pf + (double)ct.quartets * qf;
-        }
-        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
-    }
-    int slot = 0;
-    for (size_t c : order) {
+    for (size_t c = 0; c < ts->classes.size(); c++) {
         ClassTasks& ct = ts->classes[c];
-        if (ct.items.empty() && ct.items32.empty()) continue;
-        const cudaStream_t cs = fanned ? L.fan->aux[slot++ % kFan] : st;
+        if (ct.items.empty()) continue;
         a.items = ts->d_items + ct.offset;
         a.nitems = (int)ct.items.size();
-        a.counter = L.counters + c;
-        const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].first, st));
-        if (ct.compiled >= 0) {
-            const auto& e = vlx::kQuartetClasses[ct.compiled];
-            const int occ = std::max(1, e.occupancy(mode));
-            if (!ct.items.empty()) {
-                e.launch(mode, a, std::max(1, std::min(want, occ * nsm)), cs);
-                if (launches) (*launches)++;
-            }
-            if (!ct.items32.empty()) {
-                FockArgs a32 = a;
-                a32.items = ts->d_items + ct.offset32;
-                a32.nitems = (int)ct.items32.size();
-                a32.counter = L.counters + ts->classes.size() + c;
-                const int want32 = (int)((ct.items32.size() + warps_per_block - 1) / warps_per_block);
-                e.launch(mode | vlx::MODE_F32, a32, std::max(1, std::min(want32, occ * nsm)), cs);
-                if (launches) (*launches)++;
-            }
-        } else {
-            const CoopClassDev& cc = L.glob->coop[ct.coop];
-            for (int f = 0; f < 2; f++) {
-                const std::vector<WorkItem>& its = f ? ct.items32 : ct.items;
-                if (its.empty()) continue;
-                FockArgs ac = a;
-                ac.items = ts->d_items + (f ? ct.offset32 : ct.offset);
-                ac.nitems = (int)its.size();
-                ac.counter = L.counters + (f ? ts->classes.size() : 0) + c;
+        for (int f = 0; f < (ith32 >= 0 ? 2 : 1); f++) {
+            FockArgs af = a;
+            af.counter = L.counters + (f ? ts->classes.size() : 0) + c;
+            const int fmode = f ? (mode | vlx::MODE_F32) : mode;
+            if (ct.compiled >= 0) {
+                const auto& e = vlx::kQuartetClasses[ct.compiled];
+                const int occ = std::max(1, e.occupancy(mode));
+                const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
+                e.launch(fmode, af, std::max(1, std::min(want, occ * nsm)), st);
+            } else {
+                const CoopClassDev& cc = L.glob->coop[ct.coop];
                 const int wpb = vlx::coop_warps_per_block(cc, f != 0);
                 const int cap = vlx::coop_blocks_per_sm(cc, f != 0) * nsm;
-                const int grid = std::max(1, std::min((int)((its.size() + wpb - 1) / wpb), cap));
-                VLX_CUDA(vlx::launch_coop_quartet(f ? (mode | vlx::MODE_F32) : mode, ac, cc, grid, cs));
-                if (launches) (*launches)++;
+                const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
+                VLX_CUDA(vlx::launch_coop_quartet(fmode, af, cc, grid, st));
             }
+            if (launches) (*launches)++;
         }
         VLX_CUDA(cudaGetLastError());
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].second, st));
-    }
-    if (fanned) {
-        for (int i = 0; i < kFan; i++) {
-            VLX_CUDA(cudaEventRecord(L.fan->join[i], L.fan->aux[i]));
-            VLX_CUDA(cudaStreamWaitEvent(st, L.fan->join[i], 0));
-        }
     }
     return VLX_B200_OK;
 }
 
 int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
-                    double cj, double ck, double omega2, cudaStream_t st, long long* launches,
+                    double cj, double ck, double omega2, int ith, int ith32, cudaStream_t st, long long* launches,
                     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
 {
     LaunchCtx L;
@@ -798,14 +730,38 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     L.mol.F = dAcc;
     L.mol.nao = s->nao;
     for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
-    L.fan = &s->fan;
-    return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, st, launches, events);
+    return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, ith, ith32, st, launches, events);
+}
+
+// Quartets (all, FP32 part) and primitive quartets one class evaluates at the
+// run-time thresholds (the host mirror of item_range in vlx_device.cuh).
+void count_class(const vlx_b200_screener* s, const ClassTasks& ct, int ith, int ith32, long long* q,
+                 long long* q32, long long* prim)
+{
+    *q = *q32 = *prim = 0;
+    for (const WorkItem& w : ct.items) {
+        const PairBlock& Pb = s->blocks[w.blocks & 0xffff];
+        const PairBlock& Pk = s->blocks[w.blocks >> 16];
+        const int bx = Pb.bin[Pb.sorted[w.bra]];
+        const int kmax = ith - bx;
+        const int kend = (kmax < 0) ? w.kbeg : std::min(w.kend, Pk.bin_off[std::min(kmax, 15) + 1]);
+        if (kend <= w.kbeg) continue;
+        int kmid = kend;
+        if (ith32 >= 0) {
+            const int b32 = ith32 - bx;
+            const int kb32 = (b32 <= 0) ? 0 : Pk.bin_off[std::min(b32, 16)];
+            kmid = std::max(w.kbeg, std::min(kend, kb32));
+        }
+        *q += kend - w.kbeg;
+        *q32 += kend - kmid;
+        *prim += (long long)Pb.nuse[w.bra] * (Pk.nuse_prefix[kend] - Pk.nuse_prefix[w.kbeg]);
+    }
 }
 
 // Algorithmic FP64 flops of one class launch: per primitive quartet the
 // recursion graph + Boys (28 + 3M) + geometric factors (30); per contracted
 // quartet HRR + spherical transforms + digestion (12 per spherical integral).
-double class_flops(const vlx_b200_screener* s, const ClassTasks& ct)
+double class_flops(const vlx_b200_screener* s, const ClassTasks& ct, long long quartets, long long prim_quartets)
 {
     int pf = 0, qf = 0;
     if (ct.compiled >= 0) {
@@ -817,7 +773,7 @@ double class_flops(const vlx_b200_screener* s, const ClassTasks& ct)
     }
     const int M = ct.la + ct.lb + ct.lc + ct.ld;
     const double nsph = (2.0 * ct.la + 1) * (2 * ct.lb + 1) * (2 * ct.lc + 1) * (2 * ct.ld + 1);
-    return (double)ct.prim_quartets * (pf + 28 + 3 * M + 30) + (double)ct.quartets * (qf + 12.0 * nsph);
+    return (double)prim_quartets * (pf + 28 + 3 * M + 30) + (double)quartets * (qf + 12.0 * nsph);
 }
 
 int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, int symmetric, const char* label,
@@ -839,10 +795,22 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
         rc = build_tasks(s, ith, rank, nodes, &ts);
         if (rc) return rc;
         rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dD, s->d_acc, nullptr, cj,
-                             ck, omega2, st, launches);
+                             ck, omega2, ith, s->ith32, st, launches);
         if (rc) return rc;
-        if (quartets) *quartets += ts->quartets;
-        if (prim) *prim += ts->prim_quartets;
+        if (quartets || prim) {
+            long long q = ts->quartets, pq = ts->prim_quartets;
+            if (ith < ts->ith || s->ith32 >= 0) {
+                q = pq = 0;
+                for (const ClassTasks& ct : ts->classes) {
+                    long long a = 0, b = 0, c = 0;
+                    count_class(s, ct, ith, s->ith32, &a, &b, &c);
+                    q += a;
+                    pq += c;
+                }
+            }
+            if (quartets) *quartets += q;
+            if (prim) *prim += pq;
+        }
     }
     if (symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
@@ -950,8 +918,6 @@ int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, co
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) ||
         cudaEventCreate(&s->ev0) || cudaEventCreate(&s->ev1))
         return cleanup(fail(VLX_B200_ERR_CUDA, "screener_create: stream / event creation failed"));
-    rc = fan_create(&s->fan);
-    if (rc) return cleanup(rc);
     // shells and the AO map (MolecularBasis.cpp:468-490)
     size_t off = 0;
     s->shells.resize(nshells);
@@ -1051,7 +1017,6 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
-    fan_destroy(&s->fan);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return VLX_B200_OK;
@@ -1092,10 +1057,19 @@ int vlx_b200_screener_pair_info(const vlx_b200_screener* s, int* info, double* m
     return VLX_B200_OK;
 }
 
+int vlx_b200_set_work_threshold(vlx_b200_screener* s, int ithreshold_base)
+{
+    if (!s || ithreshold_base > 32) return fail(VLX_B200_ERR_ARGUMENT, "invalid work threshold");
+    s->ith_base = ithreshold_base;
+    return VLX_B200_OK;
+}
+
 int vlx_b200_set_block_size_factor(vlx_b200_screener* s, int factor)
 {
     if (!s || factor < 1) return fail(VLX_B200_ERR_ARGUMENT, "invalid block size factor");
     s->seg = std::max(32, (256 / factor) / 32 * 32);
+    s->class_seg.clear();  // the explicit knob replaces any autotuned lengths
+    s->tune_gen++;
     return VLX_B200_OK;
 }
 
@@ -1199,7 +1173,9 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
     // the work list must already exist: building it would allocate device memory
     TaskSet* ts = nullptr;
     for (auto& t : s->tasksets)
-        if (t.ith == ith && t.rank == 0 && t.nodes == 1 && t.seg == s->seg && t.ith32 < 0) ts = &t;
+        if (t.ith == std::max(ith, s->ith_base) && t.rank == 0 && t.nodes == 1 && t.seg == s->seg &&
+            t.tune_gen == s->tune_gen)
+            ts = &t;
     if (known && !ts)
         return fail(VLX_B200_ERR_ARGUMENT,
                     "fock_build_noalloc: no work list for ithreshold " + std::to_string(ith) +
@@ -1227,6 +1203,8 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
         a.cj = cj;
         a.ck = ck;
         a.omega2 = rs ? omega * omega : 0.0;
+        a.ith = ith;
+        a.ith32 = -1;
         const int mode = symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN;
         for (size_t c = 0; c < ts->classes.size(); c++) {
             const ClassTasks& ct = ts->classes[c];
@@ -1385,7 +1363,8 @@ int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
     if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     if (!rc) rc = ensure_buffers(s);
     if (!rc) rc = build_tasks(s, ith, 0, 1, &ts);
-    if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, 0.0, s->stream, nullptr);
+    if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, 0.0, ith, -1, s->stream,
+                                  nullptr);
     if (!rc) {
         e = cudaMemcpyAsync(eri_out, d_eri, bytes, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -1421,7 +1400,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
     rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, 0.0, st, nullptr, &ev);
+                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev);
     if (!rc && symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
         symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
@@ -1433,7 +1412,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     int n = 0;
     for (size_t c = 0; c < nc && !rc; c++) {
         const ClassTasks& ct = ts->classes[c];
-        if (ct.items.empty()) continue;
+        if (ct.items.empty() && ct.items32.empty()) continue;
         if (n >= max_classes) break;
         vlx_b200_class_profile& p = out[n++];
         p.la = ct.la;
@@ -1444,10 +1423,12 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
         p.device_ms = ms;
-        p.shell_quartets = ct.quartets;
-        p.prim_quartets = ct.prim_quartets;
-        p.flops = class_flops(s, ct);
-        p.fp32_quartets = ct.fp32_quartets;
+        long long q = 0, q32 = 0, pq = 0;
+        count_class(s, ct, ith, s->ith32, &q, &q32, &pq);
+        p.shell_quartets = q;
+        p.prim_quartets = pq;
+        p.flops = class_flops(s, ct, q, pq);
+        p.fp32_quartets = q32;
     }
     for (auto& x : ev) {
         cudaEventDestroy(x.first);
@@ -1568,8 +1549,8 @@ struct vlx_b200_batch {
     double* key_F = nullptr;
     int key_sym = -1, key_ith = -1;
     double key_cj = 0.0, key_ck = 0.0, key_om2 = -1.0;
+    int run_ith = 0;  // threshold of the build being enqueued
     const double* mols_D = nullptr;  // D of the uploaded per-molecule records
-    StreamFan fan;
     long long launches = 0;          // kernel launches of one build
 };
 
@@ -1663,9 +1644,8 @@ int batch_enqueue(vlx_b200_batch* b, TaskSet* ts, bool known, int symmetric, dou
         L.glob = b->glob;
         L.counters = b->d_counters;
         L.mols = b->d_mols;
-        L.fan = &b->fan;
         const int rc = enqueue_ctx(L, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, nullptr, cj, ck,
-                                   omega2, st, launches);
+                                   omega2, b->run_ith, -1, st, launches);
         if (rc) return rc;
     }
     if (symmetric) {
@@ -1723,10 +1703,6 @@ int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screen
     if (blocks.size() > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: more than 65535 pair blocks");
     VLX_CUDA(cudaSetDevice(b->device));
     VLX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    {
-        const int rc = fan_create(&b->fan);
-        if (rc) return rc;
-    }
     VLX_CUDA(cudaMalloc(&b->d_blocks, std::max<size_t>(1, blocks.size()) * sizeof(PairBlockDev)));
     if (!blocks.empty())
         VLX_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), blocks.size() * sizeof(PairBlockDev), cudaMemcpyHostToDevice));
@@ -1753,7 +1729,6 @@ int vlx_b200_batch_destroy(vlx_b200_batch* b)
     cudaFree(b->d_nao);
     cudaFree(b->d_acc);
     if (b->d_counters) cudaFree(b->d_counters);
-    fan_destroy(&b->fan);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return VLX_B200_OK;
@@ -1781,6 +1756,7 @@ int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int 
     TaskSet* ts = nullptr;
     int rc = batch_tasks(b, ith, &ts);
     if (rc) return rc;
+    b->run_ith = ith;
     if (b->mols_D != d_densities) {
         // the kernels read D and the accumulator through these records; any
         // earlier build that reads them has to finish first
@@ -1840,6 +1816,119 @@ int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int 
         stats->prim_quartets = known ? ts->prim_quartets : 0;
         stats->kernel_launches = launches;
     }
+    return VLX_B200_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ autotuning
+//
+// Per quartet class the length of the ket run of one work item (the unit of
+// the persistent work queue: long runs amortise the bra set-up, short runs
+// balance the tail of the launch) is picked by timing every class under each
+// candidate length in profiled builds (one CUDA-event pair per class launch).
+// No counterpart in the reference (its block-size factor is one global knob).
+
+namespace {
+
+struct TuneCandidate {
+    int compiled, coop;
+};
+constexpr TuneCandidate kTuneCandidates[] = {{256, 2}, {32, 1}, {64, 2}, {128, 4}, {512, 8}};
+
+}  // namespace
+
+extern "C" {
+
+int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, void* stream, int max_classes,
+                      vlx_b200_tune_result* out, int* nclasses)
+{
+    if (!s || !d_density || !out || !nclasses || max_classes < 1) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    VLX_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    int rc = ensure_buffers(s);
+    if (rc) return rc;
+    const int ith32_saved = s->ith32;
+    s->ith32 = -1;
+    s->class_seg.clear();
+    const int gen0 = ++s->tune_gen;
+    const size_t ncand = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
+    std::map<int, std::vector<float>> times;  // class key -> ms per candidate
+    std::map<int, int> kind;                  // class key -> 1 if warp-cooperative
+    double* dF = s->d_F;
+    for (size_t k = 0; k < ncand && !rc; k++) {
+        s->seg_try_compiled = kTuneCandidates[k].compiled;
+        s->seg_try_coop = kTuneCandidates[k].coop;
+        s->tune_gen = gen0 + 1 + (int)k;
+        TaskSet* ts = nullptr;
+        rc = build_tasks(s, ith, 0, 1, &ts);
+        if (rc) break;
+        const size_t nc = ts->classes.size();
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev(nc);
+        for (auto& e : ev) {
+            VLX_CUDA(cudaEventCreate(&e.first));
+            VLX_CUDA(cudaEventCreate(&e.second));
+        }
+        VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, (size_t)s->nao * s->nao * sizeof(double), st));
+        rc = enqueue_classes(s, ts, vlx::MODE_FOCK_SYM, d_density, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
+                             nullptr,
+                             &ev);
+        const cudaError_t e = cudaStreamSynchronize(st);
+        if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+        for (size_t c = 0; c < nc && !rc; c++) {
+            const ClassTasks& ct = ts->classes[c];
+            if (ct.items.empty()) continue;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
+            const int key = ct.la | (ct.lb << 4) | (ct.lc << 8) | (ct.ld << 12);
+            auto& v = times[key];
+            v.resize(ncand, 1e30f);
+            v[k] = ms;
+            kind[key] = ct.compiled < 0 ? 1 : 0;
+        }
+        for (auto& x : ev) {
+            cudaEventDestroy(x.first);
+            cudaEventDestroy(x.second);
+        }
+    }
+    (void)dF;
+    s->seg_try_compiled = s->seg_try_coop = 0;
+    // the tuning task sets are not needed any more
+    for (auto it = s->tasksets.begin(); it != s->tasksets.end();) {
+        if (it->tune_gen >= gen0) {
+            if (it->d_items) cudaFree(it->d_items);
+            it = s->tasksets.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    s->ith32 = ith32_saved;
+    if (rc) {
+        s->tune_gen++;
+        return rc;
+    }
+    int n = 0;
+    for (const auto& kv : times) {
+        const auto& v = kv.second;
+        size_t best = 0;
+        for (size_t k = 1; k < ncand; k++)
+            if (v[k] < v[best]) best = k;
+        const bool coop = kind[kv.first] != 0;
+        s->class_seg[kv.first] = coop ? kTuneCandidates[best].coop : kTuneCandidates[best].compiled;
+        if (n < max_classes) {
+            vlx_b200_tune_result& r = out[n++];
+            r.la = kv.first & 15;
+            r.lb = (kv.first >> 4) & 15;
+            r.lc = (kv.first >> 8) & 15;
+            r.ld = (kv.first >> 12) & 15;
+            r.table_driven = coop ? 1 : 0;
+            r.segment = s->class_seg[kv.first];
+            r.best_ms = v[best];
+            r.default_ms = v[0];
+        }
+    }
+    s->tune_gen++;
+    *nclasses = n;
     return VLX_B200_OK;
 }
 

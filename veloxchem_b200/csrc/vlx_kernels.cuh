@@ -212,10 +212,12 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
         const PairView bra = make_view(bb, w.bra);
         const int p0 = __ldg(bb.ao + w.bra), q0 = __ldg(bb.ao + bb.npairs + w.bra);
         const double s_bra = (p0 == q0) ? 0.5 : 1.0;
-        for (int j0 = w.kbeg; j0 < w.kend; j0 += 32) {
+        int k0, k1;
+        item_range(a, bb, kb, w, (mode & MODE_F32) != 0, k0, k1);
+        for (int j0 = k0; j0 < k1; j0 += 32) {
             const int j = j0 + lane;
-            const bool act = j < w.kend;
-            const int jj = act ? j : (w.kend - 1);
+            const bool act = j < k1;
+            const int jj = act ? j : (k1 - 1);
             const PairView ket = make_view(kb, jj);
             double f[C::NSPH];
             if (mode & MODE_F32) {

@@ -30,6 +30,8 @@ struct PairBlockDev {
     const double* ab;    // [3][npairs]  B - A
     const int* ao;       // [2][npairs]  AO index of component 0 of A and of B
     const int* nuse;     // [npairs]     primitive pairs with |kfac| >= VLX_PRIM_CUTOFF
+    const int* bin;      // [npairs]     Schwarz bin of the pair (pairs sorted by bin)
+    const int* bin_off;  // [17]         first pair of bin b (pairs with bin <= b end at bin_off[b + 1])
     int npairs;
     int kprim;
     int la, lb;
@@ -69,6 +71,8 @@ struct FockArgs {
     double* eri;              // MODE_ERI: nao^4 tensor of mol
     double cj, ck;            // J and K weights of the label
     double omega2;            // 0: Coulomb; > 0: erf(omega r)/r with omega^2 (labels j_rs, k_rs, kx_rs)
+    int ith;                  // quartets with bin_bra + bin_ket <= ith are evaluated (run-time filter)
+    int ith32;                // those with bin_bra + bin_ket >= ith32 in FP32 (-1: none)
 };
 
 }  // namespace vlx

@@ -123,11 +123,13 @@ class ScfRestrictedDriver:
         self.fp32_until_grad = 1.0e-4
         # incremental Fock builds: F_n = F_(n-1) + G(D_n - D_(n-1)) with the
         # screening threshold tightened by max|D_n - D_(n-1)| (a quartet is
-        # dropped when its Schwarz bound times max|dD| is below the dynamic
-        # threshold); a full build every rebuild_every iterations, whenever
-        # the dynamic threshold changes, and to confirm convergence
+        # dropped when its Schwarz bound times max|dD| is below a hundredth of
+        # the dynamic threshold); a full build every rebuild_every iterations,
+        # whenever the dynamic threshold changes, and to confirm convergence;
+        # after a convergence check that the full build does not confirm, the
+        # remaining iterations use full builds
         self.incremental = True
-        self.rebuild_every = 10
+        self.rebuild_every = 8
         self.history = []
         self.timings = {}
 
@@ -165,6 +167,8 @@ class ScfRestrictedDriver:
             screener = T4CScreener(device=self.device)
             screener.partition(ao_basis, molecule, 'eri')
             self.timings['screener_s'] = time.perf_counter() - t0
+        # one work list for all thresholds of this SCF (filtered at run time)
+        screener.set_work_threshold(int(round(-math.log10(self.eri_thresh))))
         if guess_density is not None:
             D = torch.as_tensor(np.asarray(guess_density), dtype=torch.float64, device=dev)
         elif self.guess in ('sad', 'learned'):
@@ -212,6 +216,7 @@ class ScfRestrictedDriver:
         converged = False
         fock_ms = 0.0
         D_prev, F2e_prev, ith_prev, since_full = None, None, -1, 0
+        incremental = self.incremental
         G = torch.empty_like(D)
 
         def evaluate(F2e):
@@ -226,7 +231,7 @@ class ScfRestrictedDriver:
             ith = int(-math.log10(self.dyn_threshold(e_grad)))
             D = 0.5 * (D + D.T).contiguous()
             mixed = self.fp32_cutoff > 0.0 and e_grad > self.fp32_until_grad
-            inc = (self.incremental and first is None and D_prev is not None and ith == ith_prev
+            inc = (incremental and first is None and D_prev is not None and ith == ith_prev
                    and since_full + 1 < self.rebuild_every)
             t0 = time.perf_counter()
             if first is not None:
@@ -236,7 +241,7 @@ class ScfRestrictedDriver:
             elif inc:
                 dD = (D - D_prev).contiguous()
                 m = float(torch.max(torch.abs(dD)))
-                ith_used = max(0, ith + math.floor(math.log10(m))) if 0.0 < m < 1.0 else ith
+                ith_used = min(ith, max(0, ith + 2 + math.floor(math.log10(m)))) if m > 0.0 else ith
                 screener.set_fp32_threshold(self.fp32_cutoff if mixed else 0.0, m)
                 build(dD, G, ith_used)
                 F2e.copy_(F2e_prev)
@@ -265,6 +270,8 @@ class ScfRestrictedDriver:
                 self.history.append({'iteration': it, 'energy': energy, 'delta_e': energy - e_old, 'e_grad': e_grad,
                                      'ithreshold': ith, 'mixed': False, 'incremental': False, 'check': True,
                                      'time_s': time.perf_counter() - t_start})
+                if e_grad >= self.conv_thresh:
+                    incremental = False
             if e_grad < self.conv_thresh:
                 converged = True
                 break

@@ -113,6 +113,11 @@ class T4CScreener:
         nat.check(nat.lib().vlx_b200_set_fp32_threshold(self.handle, float(cutoff), float(max_abs_density)),
                   'set_fp32_threshold')
 
+    def set_work_threshold(self, ithreshold_base):
+        """Build work lists for max(ithreshold, ithreshold_base) and filter at
+        run time, so builds at several thresholds share one list."""
+        nat.check(nat.lib().vlx_b200_set_work_threshold(self.handle, int(ithreshold_base)), 'set_work_threshold')
+
     def set_block_size_factor(self, factor):
         nat.check(nat.lib().vlx_b200_set_block_size_factor(self.handle, int(factor)), 'set_block_size_factor')
 
