@@ -216,6 +216,7 @@ class ScfRestrictedDriver:
         converged = False
         fock_ms = 0.0
         D_prev, F2e_prev, ith_prev, since_full = None, None, -1, 0
+        eigh_s = 0.0
         incremental = self.incremental
         G = torch.empty_like(D)
 
@@ -282,11 +283,15 @@ class ScfRestrictedDriver:
                 focks.pop(0)
                 errs.pop(0)
             F_eff = self._diis(focks, errs) if len(focks) > 1 else F
+            t0 = time.perf_counter()
             e, c = torch.linalg.eigh(X.T @ F_eff @ X)
             C = X @ c[:, :nocc]
             D = C @ C.T
+            torch.cuda.synchronize(dev)
+            eigh_s += time.perf_counter() - t0
         screener.set_fp32_threshold(0.0, 0.0)
         self.timings['fock_ms_total'] = fock_ms
+        self.timings['diag_s'] = eigh_s
         self.timings['total_s'] = time.perf_counter() - t_start
         e, c = torch.linalg.eigh(X.T @ F @ X)
         return {'scf_energy': energy, 'converged': converged,

@@ -99,6 +99,7 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
             runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
                           'converged': res['converged'], 'wall_s': time.perf_counter() - t0,
                           'fock_ms_total': res['timings']['fock_ms_total'], 'guess_used': res['guess_used'],
+                          'timings': {k: v for k, v in res['timings'].items() if isinstance(v, float)},
                           'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
                                       for h in res['history']]}
         e_ref = runs['plain_fp64_sad']['energy']
