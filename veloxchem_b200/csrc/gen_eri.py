@@ -233,7 +233,7 @@ class ClassGen:
         w('                double F[%d];' % (L + 1))
         # erf-attenuated operator: F_m(T) -> s^(2m+1) F_m(s^2 T), s^2 = om2 / (om2 + rho)
         w('                const double s2 = (om2 > 0.0) ? om2 / (om2 + rho) : 1.0;')
-        w('                boys_function<%d>(T * s2, F, btab);' % L)
+        w('                boys_function_tab<%d>(T * s2, F, btab);' % L)
         w('                double pref = kab * kcd * r;')
         w('                if (om2 > 0.0) pref *= sqrt(s2);')
         w('                #pragma unroll')
@@ -514,7 +514,7 @@ def to_f32(method_lines):
         t = t.replace('const double* __restrict__ btab', 'const float* __restrict__ btab')
         t = t.replace('double* __restrict__ out', 'float* __restrict__ out')
         t = t.replace('const double ', 'const float ').replace('double c_', 'float c_').replace('double F[', 'float F[')
-        t = t.replace('boys_function<', 'boys_function_f<').replace('rsqrt(', 'rsqrtf(')
+        t = t.replace('boys_function_tab<', 'boys_function_tab_f<').replace('rsqrt(', 'rsqrtf(')
         t = re.sub(r'(?<![r\w])sqrt\(', 'sqrtf(', t).replace('double pref', 'float pref')
         if not t.lstrip().startswith('//'):
             t = _FLOAT_LITERAL.sub(lambda m: m.group(1) + 'f', t)

@@ -197,7 +197,22 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
 {
     using C = EriClass<LA, LB, LC, LD>;
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
+    constexpr int L = LA + LB + LC + LD;
     const int lane = threadIdx.x & 31;
+    // the Boys coefficients of the one order the class needs (the lower orders
+    // follow by recursion), staged once per persistent block: the per-lane
+    // table lookups then gather from shared memory instead of L1/L2
+    __shared__ double sboys[BOYS_NINT * BOYS_NCOEF];
+    const bool f32 = (mode & MODE_F32) != 0;
+    if (f32) {
+        float* sf = reinterpret_cast<float*>(sboys);
+        for (int i = threadIdx.x; i < BOYS_NINT * BOYS_NCOEF; i += blockDim.x)
+            sf[i] = __ldg(a.boys_f + L * BOYS_NINT * BOYS_NCOEF + i);
+    } else {
+        for (int i = threadIdx.x; i < BOYS_NINT * BOYS_NCOEF; i += blockDim.x)
+            sboys[i] = __ldg(a.boys + L * BOYS_NINT * BOYS_NCOEF + i);
+    }
+    __syncthreads();
     for (;;) {
         int it = 0;
         if (lane == 0) it = atomicAdd(a.counter, 1);
@@ -220,13 +235,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
             const int jj = act ? j : (k1 - 1);
             const PairView ket = make_view(kb, jj);
             double f[C::NSPH];
-            if (mode & MODE_F32) {
+            if (f32) {
                 float g[C::NSPH];
-                C::compute_f32(bra, ket, a.boys_f, (float)a.omega2, g);
+                C::compute_f32(bra, ket, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
 #pragma unroll
                 for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
             } else {
-                C::compute(bra, ket, a.boys, a.omega2, f);
+                C::compute(bra, ket, sboys, a.omega2, f);
             }
             const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
             const int dmode = mode & 3;
@@ -256,7 +271,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(const PairBlockDev* blocks,
     if (i >= b.npairs) return;
     const PairView v = make_view(b, i);
     double f[C::NSPH];
-    C::compute(v, v, boys, 0.0, f);
+    C::compute(v, v, boys + (size_t)(2 * (LA + LB)) * BOYS_NINT * BOYS_NCOEF, 0.0, f);
     double mx = 0.0;
     for (int t = 0; t < C::NSPH; t++) mx = (f[t] > mx) ? f[t] : mx;
     maxv[i] = mx;
