@@ -201,15 +201,28 @@ class ScfRestrictedDriver:
                                                                                    S.cpu().numpy(), nocc, D_sad, X)
             self.timings['learned_guess_s'] = time.perf_counter() - t0
             ith0 = int(-math.log10(self.dyn_threshold(1.0)))
-            cands = []
-            for name, dens in (('learned', torch.from_numpy(D_l).to(dev)), ('sad', D)):
-                dens = 0.5 * (dens + dens.T).contiguous()
-                f2 = torch.empty_like(dens)
-                build(dens, f2, ith0)
-                cands.append((float(torch.sum(dens * f2) + 2.0 * torch.sum(dens * H)), name, dens, f2))
+            # the learned candidate is built as iteration 1 would build it (its
+            # F is reused there); the SAD candidate's energy only has to rank
+            # the two guesses, whose energies differ by far more than the error
+            # of a loose build (threshold 1e-6, FP32 below 1e-4: ~1e-5 Eh)
+            dl = torch.from_numpy(D_l).to(dev)
+            dl = 0.5 * (dl + dl.T).contiguous()
+            fl = torch.empty_like(dl)
+            screener.set_fp32_threshold(self.fp32_cutoff, float(torch.max(torch.abs(dl))))
+            build(dl, fl, ith0)
+            ds = 0.5 * (D + D.T).contiguous()
+            fs = torch.empty_like(ds)
+            screener.set_fp32_threshold(1.0e-4, float(torch.max(torch.abs(ds))))
+            build(ds, fs, min(ith0, 6))
+            screener.set_fp32_threshold(0.0, 0.0)
+            e_l = float(torch.sum(dl * fl) + 2.0 * torch.sum(dl * H))
+            e_s = float(torch.sum(ds * fs) + 2.0 * torch.sum(ds * H))
             torch.cuda.synchronize(dev)
-            e_best, self.guess_used, D, first = min(cands, key=lambda c: c[0])
-            self.timings['guess_energies'] = {c[1]: c[0] + e_nuc for c in cands}
+            if e_l <= e_s:
+                self.guess_used, D, first = 'learned', dl, fl
+            else:
+                self.guess_used, D = 'sad', ds
+            self.timings['guess_energies'] = {'learned': e_l + e_nuc, 'sad': e_s + e_nuc}
         focks, errs = [], []
         e_grad, energy, e_old = 1.0, 0.0, 0.0
         self.history = []
