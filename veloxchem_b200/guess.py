@@ -257,11 +257,13 @@ class LearnedGuessDriver:
         self.net.load_state_dict(data)
         self.device = device
 
-    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None, ortho=None):
+    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None, ortho=None, refine_grad=1.0e-3):
         """Learned alpha density in `basis`: predicted in def2-SVP and, for any
-        other basis, carried over by the standard basis projection
-        D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis, s: def2-SVP)
-        before the idempotent projection."""
+        other basis, first refined by a loose def2-SVP SCF started from the
+        prediction (electronic gradient below refine_grad; mixed precision,
+        incremental builds), then carried over by the standard basis
+        projection D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis,
+        s: def2-SVP) before the idempotent projection."""
         import torch
         from . import _native as nat
         from .molecularbasis import MolecularBasis
@@ -274,6 +276,13 @@ class LearnedGuessDriver:
         d_svp = self.predict(molecule, svp, SadGuessDriver().compute(molecule, minb, svp, self.device), s_svp, nocc)
         if basis.name.upper() == 'DEF2-SVP':
             return d_svp
+        if refine_grad:
+            from .scf import ScfRestrictedDriver
+            drv = ScfRestrictedDriver(self.device)
+            drv.conv_thresh = refine_grad
+            drv.fp32_cutoff = 1.0e-5
+            res = drv.compute(molecule, svp, guess_density=d_svp)
+            d_svp = res['D_alpha']
         dev = self.net.dev
         s_bs = torch.as_tensor(nat.one_electron(0, molecule, basis, svp, self.device), device=dev)
         s_bb = torch.as_tensor(overlap, dtype=torch.float64, device=dev)

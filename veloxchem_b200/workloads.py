@@ -49,7 +49,7 @@ def _build_ms(scr, d, f, reps=3):
     return best
 
 
-def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
+def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=True):
     from . import T4CScreener
     from . import _native as nat
     from .geometry import random_density
@@ -61,7 +61,9 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
     d = torch.from_numpy(random_density(scr.nao, 320, 1)).cuda()
     f64 = torch.empty_like(d)
     out = {'workload': '(H2O)64 / def2-TZVP, 2J-K, ithreshold 12', 'nao': scr.nao}
-    t64 = _build_ms(scr, d, f64)
+    if not builds:
+        cutoffs = ()
+    t64 = _build_ms(scr, d, f64, reps=3 if builds else 0)
     prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
     flops = sum(p['flops'] for p in prof)
     out['fp64'] = {'build_ms': t64, 'flops': flops, 'tflops': flops / t64 / 1e9,
@@ -90,6 +92,8 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
                                       ('mixed_1e-6_sad', 1e-6, 'sad', False),
                                       ('fp64_learned', 0.0, 'learned', False),
                                       ('mixed_learned_incremental', 1e-6, 'learned', True)):
+            if variants and name not in variants:
+                continue
             drv = ScfRestrictedDriver()
             drv.fp32_cutoff = cut
             drv.guess = guess
@@ -102,7 +106,8 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True):
                           'timings': {k: v for k, v in res['timings'].items() if isinstance(v, float)},
                           'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
                                       for h in res['history']]}
-        e_ref = runs['plain_fp64_sad']['energy']
+        # E_ref: the plain FP64 run (or, if it was not run, the last variant's energy)
+        e_ref = runs['plain_fp64_sad']['energy'] if 'plain_fp64_sad' in runs else list(runs.values())[-1]['energy']
         for r in runs.values():
             r['energy_error'] = r['energy'] - e_ref
             r['time_to_1e-6_s'] = next((h[3] for k, h in enumerate(r['history'])
@@ -218,11 +223,14 @@ def main(argv=None):
     ap.add_argument('--basis', default='def2-tzvp')
     ap.add_argument('--repeat', type=int, default=1)
     ap.add_argument('--fp32-cutoff', type=float, default=0.0)
+    ap.add_argument('--scf-variants', default=None, help='comma-separated subset of the C3 SCF variants')
+    ap.add_argument('--no-builds', action='store_true', help='C3: skip the per-cutoff build table')
     a = ap.parse_args(argv)
     if a.which == 'build':
         res = build(a.cluster, a.basis, a.repeat, a.fp32_cutoff)
     else:
-        res = c3(scf=not a.no_scf) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf())
+        res = (c3(scf=not a.no_scf, variants=a.scf_variants.split(',') if a.scf_variants else None,
+                  builds=not a.no_builds) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf()))
     text = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, 'w') as fh:
