@@ -257,13 +257,15 @@ class LearnedGuessDriver:
         self.net.load_state_dict(data)
         self.device = device
 
-    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None, ortho=None, refine_grad=1.0e-3):
+    def predict_any(self, molecule, basis, overlap, nocc, sad_density=None, ortho=None, refine_grad=None):
         """Learned alpha density in `basis`: predicted in def2-SVP and, for any
-        other basis, first refined by a loose def2-SVP SCF started from the
-        prediction (electronic gradient below refine_grad; mixed precision,
-        incremental builds), then carried over by the standard basis
-        projection D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis,
-        s: def2-SVP) before the idempotent projection."""
+        other basis, carried over by the standard basis projection
+        D = S_bb^-1 S_bs D_svp S_sb S_bb^-1 (b: target basis, s: def2-SVP)
+        before the idempotent projection.  With refine_grad, the prediction is
+        first refined by a loose def2-SVP SCF (gradient below refine_grad);
+        measured on (H2O)64 / def2-TZVP this improved the first-iteration
+        energy only from 3.0 to 2.7 Eh above the converged one for 3.6 s, so
+        it is off by default."""
         import torch
         from . import _native as nat
         from .molecularbasis import MolecularBasis
