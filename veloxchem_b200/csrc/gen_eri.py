@@ -569,13 +569,13 @@ def emit_class_file(cls, outdir):
     w('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st)' % nm)
     w('{')
     w('    const dim3 blk(32 * kWarpsPerBlock);')
-    w('    quartet_kernel<%d, %d, %d, %d><<<grid, blk, 0, st>>>(a, mode);' % cls)
+    w('    quartet_kernel_of<%d, %d, %d, %d>()<<<grid, blk, 0, st>>>(a, mode);' % cls)
     w('}')
     w('int occupancy_quartet_%s(int mode)' % nm)
     w('{')
     w('    int n = 0;')
     w('    (void)mode;')
-    w('    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel<%d, %d, %d, %d>, 32 * kWarpsPerBlock, 0);' % cls)
+    w('    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel_of<%d, %d, %d, %d>(), 32 * kWarpsPerBlock, 0);' % cls)
     w('    return n;')
     w('}')
     if (la, lb) == (lc, ld):

@@ -192,8 +192,21 @@ __device__ __forceinline__ void scatter_eri(const double* f, const int p0, const
 
 constexpr int kWarpsPerBlock = 4;
 
+// Classes compiled with a minimum of 4 resident 128-thread blocks per SM:
+// their unconstrained allocation (164-168 registers, 3 blocks) fits 128
+// registers without spilling.  (An explicit minimum of 1 is not the same as
+// none: it lets the compiler take far more registers, e.g. 186 instead of 72
+// for (sp|ss), so the other classes keep the plain bound.)
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const FockArgs a, const int mode)
+struct FourBlocks {
+    static constexpr bool value = false;
+};
+template <> struct FourBlocks<1, 1, 0, 0> { static constexpr bool value = true; };
+template <> struct FourBlocks<1, 1, 0, 1> { static constexpr bool value = true; };
+template <> struct FourBlocks<0, 2, 0, 1> { static constexpr bool value = true; };
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
 {
     using C = EriClass<LA, LB, LC, LD>;
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
@@ -258,6 +271,28 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
             }
         }
     }
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const FockArgs a, const int mode)
+{
+    quartet_body<LA, LB, LC, LD>(a, mode);
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 4) quartet_kernel_b4(const FockArgs a, const int mode)
+{
+    quartet_body<LA, LB, LC, LD>(a, mode);
+}
+
+// the kernel variant of a class
+template <int LA, int LB, int LC, int LD>
+constexpr auto quartet_kernel_of()
+{
+    if constexpr (FourBlocks<LA, LB, LC, LD>::value)
+        return &quartet_kernel_b4<LA, LB, LC, LD>;
+    else
+        return &quartet_kernel<LA, LB, LC, LD>;
 }
 
 // max over all spherical components of (ab|ab) per pair (T4CScreener::partition)
