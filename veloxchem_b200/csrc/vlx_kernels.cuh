@@ -192,18 +192,19 @@ __device__ __forceinline__ void scatter_eri(const double* f, const int p0, const
 
 constexpr int kWarpsPerBlock = 4;
 
-// Classes compiled with a minimum of 4 resident 128-thread blocks per SM:
-// their unconstrained allocation (164-168 registers, 3 blocks) fits 128
-// registers without spilling.  (An explicit minimum of 1 is not the same as
-// none: it lets the compiler take far more registers, e.g. 186 instead of 72
-// for (sp|ss), so the other classes keep the plain bound.)
+// Minimum resident 128-thread blocks per SM a class's register allocation
+// must allow (0: no minimum).  4 for classes whose unconstrained allocation
+// (164-168 registers, 3 blocks) fits 128 registers without spilling (measured:
+// 15-20% faster each); a minimum of 3 for the classes at 250+ registers was
+// measured neutral.  An explicit minimum of 1 is not the same as none: it
+// lets the compiler take far more registers (186 instead of 72 for (sp|ss)).
 template <int LA, int LB, int LC, int LD>
-struct FourBlocks {
-    static constexpr bool value = false;
+struct BlocksHint {
+    static constexpr int value = 0;
 };
-template <> struct FourBlocks<1, 1, 0, 0> { static constexpr bool value = true; };
-template <> struct FourBlocks<1, 1, 0, 1> { static constexpr bool value = true; };
-template <> struct FourBlocks<0, 2, 0, 1> { static constexpr bool value = true; };
+template <> struct BlocksHint<1, 1, 0, 0> { static constexpr int value = 4; };
+template <> struct BlocksHint<1, 1, 0, 1> { static constexpr int value = 4; };
+template <> struct BlocksHint<0, 2, 0, 1> { static constexpr int value = 4; };
 
 template <int LA, int LB, int LC, int LD>
 __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
@@ -279,8 +280,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const Fock
     quartet_body<LA, LB, LC, LD>(a, mode);
 }
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock, 4) quartet_kernel_b4(const FockArgs a, const int mode)
+template <int MB, int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, MB) quartet_kernel_mb(const FockArgs a, const int mode)
 {
     quartet_body<LA, LB, LC, LD>(a, mode);
 }
@@ -289,8 +290,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 4) quartet_kernel_b4(cons
 template <int LA, int LB, int LC, int LD>
 constexpr auto quartet_kernel_of()
 {
-    if constexpr (FourBlocks<LA, LB, LC, LD>::value)
-        return &quartet_kernel_b4<LA, LB, LC, LD>;
+    constexpr int mb = BlocksHint<LA, LB, LC, LD>::value;
+    if constexpr (mb > 0)
+        return &quartet_kernel_mb<(mb > 0 ? mb : 1), LA, LB, LC, LD>;
     else
         return &quartet_kernel<LA, LB, LC, LD>;
 }
