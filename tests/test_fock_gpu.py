@@ -303,3 +303,31 @@ def test_shared_work_list_filters_thresholds_at_run_time():
     for ith in (4, 8, 12, 15):
         f = _fock(s, g['density'], '2jk', 1.0, ith)
         assert np.max(np.abs(f - ref.fock(g['density'], '2jk', 1.0, ith))) < TOL, ith
+
+
+@pytest.mark.parametrize('xyz,basis', [('H 0.0 0.0 0.0', 'sto-3g'),
+                                       ('He 0.0 0.0 0.0\nHe 0.0 0.0 50.0', 'def2-svp'),
+                                       ('H 0.0 0.0 0.0\nH 0.0 0.0 0.74', 'def2-tzvp')])
+def test_edge_systems_against_oracle(xyz, basis):
+    """Smallest systems: one function; two atoms 50 Angstrom apart (every
+    cross pair screened out); a molecule with only H shells up to p."""
+    from oracle.oracle import PortOracle
+    from veloxchem_b200 import MolecularBasis, Molecule
+    mol = Molecule.read_str(xyz)
+    bas = MolecularBasis.read(mol, basis)
+    s = _screener(mol, bas)
+    rng = np.random.default_rng(1)
+    c = rng.standard_normal((s.nao, max(1, s.nao // 2)))
+    d = c @ c.T / s.nao
+    for label in ('2jk', 'j', 'k'):
+        ref = PortOracle(mol, bas).fock(d, label, 1.0, 15)
+        assert np.max(np.abs(_fock(s, d, label, 1.0, 15) - ref)) < TOL, label
+
+
+def test_threshold_zero_keeps_only_the_largest_quartets():
+    from oracle.oracle import PortOracle
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    f = _fock(s, g['density'], '2jk', 1.0, 0)
+    assert np.max(np.abs(f - PortOracle(mol, bas).fock(g['density'], '2jk', 1.0, 0))) < TOL
+    assert np.max(np.abs(f)) > 0.0

@@ -112,6 +112,8 @@ def _loop_descriptors(lay):
         v = v @ lay.frames[lay.water[i]]
         g = np.exp(-((d[mask][:, None] - MOM_CENTERS[None, :]) / MOM_WIDTH) ** 2)
         out.append((g[:, :, None] * v[:, None, :]).sum(axis=0).ravel())
+        q = (g[:, :, None, None] * v[:, None, :, None] * v[:, None, None, :]).sum(axis=0)
+        out.append(np.stack([q[:, 0, 0], q[:, 1, 1], q[:, 2, 2], q[:, 0, 1], q[:, 0, 2], q[:, 1, 2]], axis=1).ravel())
         return np.concatenate(out)
 
     e = [env(i) for i in range(len(lay.z))]

@@ -302,9 +302,8 @@ struct ClassTasks {
     int coop = -1;      // index into DeviceGlobals::coop
     int la = 0, lb = 0, lc = 0, ld = 0;
     std::vector<WorkItem> items;    // FP64 quartets
-    std::vector<WorkItem> items32;  // unused (the FP32 part of an item is selected at run time)
-    size_t offset = 0, offset32 = 0;
-    long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0, fp32_quartets = 0;
+    size_t offset = 0;  // first item in the task set's device array
+    long long quartets = 0, prim_quartets = 0, ref_prim_quartets = 0;  // at the task set's threshold
 };
 
 struct TaskSet {
@@ -589,15 +588,13 @@ int build_tasks(vlx_b200_screener* s, int ith_req, int rank, int nodes, TaskSet*
     for (auto& ct : ts.classes) {
         ct.offset = total;
         total += ct.items.size();
-        ct.offset32 = total;
-        total += ct.items32.size();
     }
     if (total > 0) {
         std::vector<WorkItem> all;
         all.reserve(total);
         for (auto& ct : ts.classes) {
             all.insert(all.end(), ct.items.begin(), ct.items.end());
-            all.insert(all.end(), ct.items32.begin(), ct.items32.end());
+
         }
         VLX_CUDA(cudaMalloc(&ts.d_items, total * sizeof(WorkItem)));
         VLX_CUDA(cudaMemcpy(ts.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));
@@ -1412,7 +1409,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     int n = 0;
     for (size_t c = 0; c < nc && !rc; c++) {
         const ClassTasks& ct = ts->classes[c];
-        if (ct.items.empty() && ct.items32.empty()) continue;
+        if (ct.items.empty()) continue;
         if (n >= max_classes) break;
         vlx_b200_class_profile& p = out[n++];
         p.la = ct.la;
@@ -1587,19 +1584,14 @@ int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
                 m.classes.push_back(std::move(n));
             }
             ClassTasks& d = m.classes[it->second];
-            for (int f = 0; f < 2; f++) {
-                const std::vector<WorkItem>& src = f ? ct.items32 : ct.items;
-                std::vector<WorkItem>& dst = f ? d.items32 : d.items;
-                for (WorkItem w : src) {
-                    const int bb = (w.blocks & 0xffff) + boff, kb = (w.blocks >> 16) + boff;
-                    w.blocks = bb | (kb << 16);
-                    dst.push_back(w);
-                }
+            for (WorkItem w : ct.items) {
+                const int bb = (w.blocks & 0xffff) + boff, kb = (w.blocks >> 16) + boff;
+                w.blocks = bb | (kb << 16);
+                d.items.push_back(w);
             }
             d.quartets += ct.quartets;
             d.prim_quartets += ct.prim_quartets;
             d.ref_prim_quartets += ct.ref_prim_quartets;
-            d.fp32_quartets += ct.fp32_quartets;
         }
         m.quartets += t->quartets;
         m.prim_quartets += t->prim_quartets;
@@ -1609,15 +1601,13 @@ int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
     for (auto& ct : m.classes) {
         ct.offset = total;
         total += ct.items.size();
-        ct.offset32 = total;
-        total += ct.items32.size();
     }
     if (total > 0) {
         std::vector<WorkItem> all;
         all.reserve(total);
         for (auto& ct : m.classes) {
             all.insert(all.end(), ct.items.begin(), ct.items.end());
-            all.insert(all.end(), ct.items32.begin(), ct.items32.end());
+
         }
         VLX_CUDA(cudaMalloc(&m.d_items, total * sizeof(WorkItem)));
         VLX_CUDA(cudaMemcpy(m.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));

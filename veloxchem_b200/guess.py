@@ -15,8 +15,8 @@ where R_i is the block-diagonal rotation of the real solid harmonics of atom
 i's shells for that frame.  B_ij is invariant under rigid rotations and
 translations of the cluster, and so is the pair descriptor: element pair,
 distance, the pair vector and relative orientation in the two frames, the
-atoms' positions in their waters, and radial (and first-moment) neighbour
-densities within 5 Angstrom.  The network predicts B_ij - B_ij(SAD) for all
+atoms' positions in their waters, and radial neighbour densities and the
+first and second moments of the neighbour directions within 5 Angstrom.  The network predicts B_ij - B_ij(SAD) for all
 pairs closer than PAIR_CUTOFF; blocks beyond it are zero.  The assembled
 matrix is symmetrised and replaced by the nearest idempotent density with
 N_occ electrons (its N_occ natural orbitals of largest occupation).
@@ -39,7 +39,8 @@ MOM_CENTERS = np.array([1.5, 2.5, 3.5, 4.5])
 MOM_WIDTH = 0.7
 NTYPES = 5              # self-O, self-H, O-O, O-H, H-H
 NOUT = 196              # largest block: O x O in def2-SVP (14 x 14)
-NFEAT = NTYPES + 1 + 3 + 3 + 3 + 9 + 3 + 3 + 2 * 2 * len(RBF_CENTERS) + 2 * 3 * len(MOM_CENTERS)
+NENV = 2 * len(RBF_CENTERS) + 3 * len(MOM_CENTERS) + 6 * len(MOM_CENTERS)  # per atom
+NFEAT = NTYPES + 1 + 3 + 3 + 3 + 9 + 3 + 3 + 2 * NENV
 
 WEIGHTS = Path(__file__).resolve().parent / 'data' / 'guess_mlp_svp.npz'
 
@@ -169,7 +170,9 @@ class ClusterLayout:
 
     # ---- descriptors
     def _env_all(self):
-        """Radial O / H neighbour densities and first moments (local frame) of every atom."""
+        """Radial O / H neighbour densities and the first and second moments
+        (local frame; xx, yy, zz, xy, xz, yz) of the neighbour directions of
+        every atom."""
         d = self.dist
         mask = (d > 1e-8) & (d < ENV_CUTOFF)
         out = []
@@ -182,6 +185,9 @@ class ClusterLayout:
         v = np.einsum('ink,ikl->inl', v, self.frames[self.water])                    # local frame of i
         g = np.exp(-((d[:, :, None] - MOM_CENTERS[None, None, :]) / MOM_WIDTH) ** 2) * mask[:, :, None]
         out.append(np.einsum('inc,inl->icl', g, v).reshape(len(self.z), -1))
+        q = np.einsum('inc,inl,inm->iclm', g, v, v)
+        iu = ([0, 1, 2, 0, 0, 1], [0, 1, 2, 1, 2, 2])
+        out.append(q[:, :, iu[0], iu[1]].reshape(len(self.z), -1))
         return np.concatenate(out, axis=1)
 
     def descriptors(self):

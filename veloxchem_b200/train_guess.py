@@ -7,8 +7,9 @@
    is converged with this package's FP64 SCF from SAD; the pair descriptors
    and the local-frame blocks of (D_converged - D_SAD) are the samples.
 2. Training: the three-layer network of guess_net.GuessMLP (width 128, SiLU),
-   FP32, masked mean squared error, Adam with cosine-decayed step size, all
-   through the library's own kernels; 5% of the clusters are held out.
+   FP32, masked mean squared error (on-site blocks weighted SELF_WEIGHT),
+   Adam with cosine-decayed step size, all through the library's own
+   kernels; 5% of the clusters are held out.
 3. Evaluation: held-out (H2O)_n clusters on a 4 x 4 x 3 lattice, SCF from SAD
    and from the learned guess (with the SAD fallback of the SCF driver);
    reports iterations and time to |E - E_ref| < 1e-6 Eh, E_ref being the FP64
@@ -21,6 +22,8 @@ import math
 import time
 
 import numpy as np
+
+SELF_WEIGHT = 10.0  # loss weight of the on-site (i = j) blocks
 
 
 def _scf(mol, bas, guess, conv=1e-6, weights=None, guess_density=None, incremental=True):
@@ -58,6 +61,8 @@ def generate(clusters, nmin, nmax, seed, log=print):
         ts, _ = lay.local_blocks(d_sad)
         X.append(lay.descriptors())
         T.append(tc - ts)
+        # on-site blocks weigh more: the energy is most sensitive to them
+        m[lay.pairs[:, 0] == lay.pairs[:, 1]] *= SELF_WEIGHT
         M.append(m)
         owner.append(np.full(len(lay.pairs), c, dtype=np.int64))
         if (c + 1) % 100 == 0:
@@ -65,7 +70,7 @@ def generate(clusters, nmin, nmax, seed, log=print):
     return np.concatenate(X), np.concatenate(T), np.concatenate(M), np.concatenate(owner)
 
 
-def train(X, T, M, owner, epochs=60, batch=4096, lr=2e-3, scale=10.0, seed=0, log=print):
+def train(X, T, M, owner, epochs=120, batch=4096, lr=2e-3, scale=10.0, seed=0, log=print):
     import torch
     from .guess import NFEAT, NOUT
     from .guess_net import GuessMLP
@@ -160,7 +165,7 @@ def main(argv=None):
     ap.add_argument('--nmin', type=int, default=2)
     ap.add_argument('--nmax', type=int, default=24)
     ap.add_argument('--seed', type=int, default=100000)
-    ap.add_argument('--epochs', type=int, default=60)
+    ap.add_argument('--epochs', type=int, default=120)
     ap.add_argument('--out', default='guess_mlp_svp.npz')
     ap.add_argument('--eval', type=int, default=100)
     ap.add_argument('--eval-waters', type=int, default=48)
