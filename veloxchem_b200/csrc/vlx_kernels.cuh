@@ -203,6 +203,9 @@ struct BlocksHint {
     static constexpr int value = 0;
 };
 template <> struct BlocksHint<1, 1, 0, 0> { static constexpr int value = 4; };
+template <> struct BlocksHint<0, 1, 0, 1> { static constexpr int value = 5; };
+template <> struct BlocksHint<0, 2, 0, 0> { static constexpr int value = 5; };
+template <> struct BlocksHint<0, 1, 0, 0> { static constexpr int value = 8; };
 template <> struct BlocksHint<1, 1, 0, 1> { static constexpr int value = 4; };
 template <> struct BlocksHint<0, 2, 0, 1> { static constexpr int value = 4; };
 
