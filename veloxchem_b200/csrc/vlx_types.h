@@ -13,10 +13,11 @@
 #define BOYS_NCOEF 10
 
 // Primitive pairs whose prefactor N_a N_b S_ab sqrt(zeta) (2/sqrt(pi))^{1/2}
-// is below this bound are skipped: their contribution to any integral is below
-// 1e-24 times the partner pair's prefactor and the recursion factors, i.e. far
-// below double-precision resolution of the contracted integrals.
-#define VLX_PRIM_CUTOFF 1e-24
+// is below this bound are skipped: a primitive quartet contributes at most the
+// product of its two pair prefactors times 1/sqrt(zeta + eta), F_m <= 1 and
+// the recursion factors, and pair prefactors are at most ~5 for normalised
+// shells, so a skipped pair changes any integral by well under 1e-15.
+#define VLX_PRIM_CUTOFF 1e-18
 
 // Highest angular momentum per shell compiled into the class kernels.
 #define VLX_LMAX 3
