@@ -275,7 +275,8 @@ def run_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e = {'value': world * ne2e / float(te.item()), 'unit': UNIT, 'h2d_bytes_per_step': nao * nao * 8,
            'd2h_bytes_per_step': nao * nao * 8,
-           'path': 'FockDriver.compute(screener, Matrix, "2jk", 1.0, 0.0, 12): host density in, host Fock out'}
+           'path': 'FockDriver.compute(screener, Matrix, "2jk", 1.0, 0.0, 12): host Matrix in, host Matrix out; '
+                   'the copies go through page-locked staging buffers of the driver'}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

@@ -46,6 +46,21 @@ class _FockDriver:
     def __init__(self):
         self._bsf = None
         self.last_stats = None
+        self._stage = None  # page-locked host staging buffers (density in, Fock out)
+
+    def _staging(self, n):
+        """Page-locked nao x nao host buffers for the copies to and from the
+        GPU (allocated once per size through torch; plain host memory where
+        torch cannot pin it)."""
+        if self._stage is None or self._stage[0].shape != (n, n):
+            try:
+                import torch
+                ti = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+                to = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+                self._stage = (ti.numpy(), to.numpy(), ti, to)
+            except (RuntimeError, ImportError):
+                self._stage = (np.empty((n, n)), np.empty((n, n)), None, None)
+        return self._stage[0], self._stage[1]
 
     def _set_block_size_factor(self, factor):
         self._bsf = int(factor)
@@ -60,9 +75,10 @@ class _FockDriver:
         if dense.shape != (screener.nao, screener.nao):
             raise ValueError('FockDriver: density is %s, basis has %d functions' % (dense.shape, screener.nao))
         symmetric = int(density.get_type() == mat_t.symmetric)
-        out = np.zeros_like(dense)
+        din, out = self._staging(dense.shape[0])
+        din[:, :] = dense
         st = nat.Stats()
-        nat.check(nat.lib().vlx_b200_fock_build_local(screener.handle, int(rank), int(nodes), nat.dptr(dense),
+        nat.check(nat.lib().vlx_b200_fock_build_local(screener.handle, int(rank), int(nodes), nat.dptr(din),
                                                        symmetric, label.encode(), float(exchange_factor),
                                                        float(omega), int(ithreshold), nat.dptr(out),
                                                        ctypes.byref(st)), 'fock_build')
