@@ -1664,6 +1664,8 @@ void batch_release_graph(vlx_b200_batch* b)
 
 extern "C" {
 
+int vlx_b200_batch_destroy(vlx_b200_batch* b);
+
 int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screeners, int n)
 {
     if (!out || !screeners || n < 1 || n > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: bad arguments");
@@ -1691,17 +1693,27 @@ int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screen
         }
     }
     if (blocks.size() > 65535) return fail(VLX_B200_ERR_ARGUMENT, "batch_create: more than 65535 pair blocks");
-    VLX_CUDA(cudaSetDevice(b->device));
-    VLX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-    VLX_CUDA(cudaMalloc(&b->d_blocks, std::max<size_t>(1, blocks.size()) * sizeof(PairBlockDev)));
-    if (!blocks.empty())
-        VLX_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), blocks.size() * sizeof(PairBlockDev), cudaMemcpyHostToDevice));
-    VLX_CUDA(cudaMalloc(&b->d_mols, n * sizeof(vlx::MolDev)));
-    VLX_CUDA(cudaMalloc(&b->d_off, (n + 1) * sizeof(long long)));
-    VLX_CUDA(cudaMemcpy(b->d_off, b->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
-    VLX_CUDA(cudaMalloc(&b->d_nao, n * sizeof(int)));
-    VLX_CUDA(cudaMemcpy(b->d_nao, nao.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    VLX_CUDA(cudaMalloc(&b->d_acc, (size_t)std::max<long long>(b->off.back(), 1) * sizeof(double)));
+    // device set-up; on failure everything made so far is released
+    auto setup = [&]() -> int {
+        VLX_CUDA(cudaSetDevice(b->device));
+        VLX_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        VLX_CUDA(cudaMalloc(&b->d_blocks, std::max<size_t>(1, blocks.size()) * sizeof(PairBlockDev)));
+        if (!blocks.empty())
+            VLX_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), blocks.size() * sizeof(PairBlockDev),
+                                cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMalloc(&b->d_mols, n * sizeof(vlx::MolDev)));
+        VLX_CUDA(cudaMalloc(&b->d_off, (n + 1) * sizeof(long long)));
+        VLX_CUDA(cudaMemcpy(b->d_off, b->off.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMalloc(&b->d_nao, n * sizeof(int)));
+        VLX_CUDA(cudaMemcpy(b->d_nao, nao.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+        VLX_CUDA(cudaMalloc(&b->d_acc, (size_t)std::max<long long>(b->off.back(), 1) * sizeof(double)));
+        return VLX_B200_OK;
+    };
+    const int rc = setup();
+    if (rc) {
+        vlx_b200_batch_destroy(b.release());
+        return rc;
+    }
     *out = b.release();
     return VLX_B200_OK;
 }
