@@ -349,6 +349,14 @@ struct vlx_b200_screener {
 
 namespace {
 
+// Byte offset of a pair block's FP32 fields (after its FP64 fields and index
+// arrays, 16-byte aligned).
+size_t fp32_offset(size_t n, size_t kp)
+{
+    const size_t bytes = (9 * kp * n + 3 * n) * sizeof(double) + (4 * n + 17) * sizeof(int);
+    return (bytes + 15) & ~size_t(15);
+}
+
 // Builds device arrays of all pair blocks; `sorted` selects the screened,
 // bin-sorted pair order instead of the reference order.
 int upload_pairs(vlx_b200_screener* s, bool sorted)
@@ -361,7 +369,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         const size_t n = sorted ? pb.sorted.size() : pb.pairs.size();
         npairs[b] = (int)n;
         const size_t k = (size_t)pb.ka * pb.kb;
-        size_t bytes = (9 * k * n + 3 * n) * sizeof(double) + (4 * n + 17) * sizeof(int);
+        size_t bytes = fp32_offset(n, k) + (9 * k * n + 3 * n) * sizeof(float);
         bytes = (bytes + 255) & ~size_t(255);
         offs[b + 1] = offs[b] + bytes;
     }
@@ -379,6 +387,8 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         int* nuse = ao + 2 * n;
         int* bins = nuse + n;     // Schwarz bin per pair (sorted order; 0 before screening)
         int* bin_off = bins + n;  // first pair of bin >= b (17 entries)
+        float* primf = reinterpret_cast<float*>(host.data() + offs[b] + fp32_offset(n, (size_t)kp));
+        float* abf = primf + 9 * (size_t)kp * n;
         for (int k = 0; k <= 16; k++) bin_off[k] = sorted ? pb.bin_off[k] : 0;
         for (size_t i = 0; i < n; i++) {
             bins[i] = sorted ? pb.bin[pb.sorted[i]] : 0;
@@ -388,6 +398,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
             double r2 = 0.0;
             for (int x = 0; x < 3; x++) {
                 ab[x * n + i] = B.xyz[x] - A.xyz[x];
+                abf[x * n + i] = (float)ab[x * n + i];
                 r2 += (B.xyz[x] - A.xyz[x]) * (B.xyz[x] - A.xyz[x]);
             }
             ao[i] = A.ao0;
@@ -419,7 +430,10 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
             nuse[i] = std::max(used, 1);
             if (sorted) s->blocks[b].nuse[i] = nuse[i];
             for (int p = 0; p < kp; p++)
-                for (int f = 0; f < 9; f++) prim[((size_t)f * kp + p) * n + i] = vals[p][f];
+                for (int f = 0; f < 9; f++) {
+                    prim[((size_t)f * kp + p) * n + i] = vals[p][f];
+                    primf[((size_t)f * kp + p) * n + i] = (float)vals[p][f];
+                }
         }
     }
     if (sorted)
@@ -438,6 +452,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         PairBlockDev d;
         d.prim = reinterpret_cast<const double*>(s->d_pairs + offs[b]);
         d.ab = d.prim + 9 * (size_t)kp * n;
+        d.primf = reinterpret_cast<const float*>(s->d_pairs + offs[b] + fp32_offset(n, (size_t)kp));
         d.ao = reinterpret_cast<const int*>(d.ab + 3 * n);
         d.nuse = d.ao + 2 * n;
         d.bin = d.nuse + n;

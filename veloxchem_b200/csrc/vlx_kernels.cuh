@@ -254,7 +254,8 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
             double f[C::NSPH];
             if (f32) {
                 float g[C::NSPH];
-                C::compute_f32(bra, ket, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
+                const PairViewF braf = make_view_f(bb, w.bra, bra.kuse), ketf = make_view_f(kb, jj, ket.kuse);
+                C::compute_f32(braf, ketf, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
 #pragma unroll
                 for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
             } else {

@@ -29,6 +29,7 @@ namespace vlx {
 struct PairBlockDev {
     const double* prim;  // [9][kprim][npairs], per pair sorted by |kfac| descending
     const double* ab;    // [3][npairs]  B - A
+    const float* primf;  // [9][kprim][npairs] prim rounded to FP32, then [3][npairs] ab (mixed-precision kernels)
     const int* ao;       // [2][npairs]  AO index of component 0 of A and of B
     const int* nuse;     // [npairs]     primitive pairs with |kfac| >= VLX_PRIM_CUTOFF
     const int* bin;      // [npairs]     Schwarz bin of the pair (pairs sorted by bin)

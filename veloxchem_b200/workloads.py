@@ -82,7 +82,9 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=T
         n32 = sum(p['fp32_quartets'] for p in prof)
         nq = sum(p['shell_quartets'] for p in prof)
         out['mixed'].append({'cutoff': cut, 'build_ms': tm, 'speedup': t64 / tm, 'fp32_share': n32 / max(nq, 1),
-                             'max_abs_fock_error': float((fm - f64).abs().max())})
+                             'max_abs_fock_error': float((fm - f64).abs().max()),
+                             'class_ms': {'%d%d%d%d' % (p['la'], p['lb'], p['lc'], p['ld']): p['device_ms']
+                                          for p in prof}})
     scr.set_fp32_threshold(0.0, 0.0)
     if scf:
         runs = {}
