@@ -146,3 +146,25 @@ def test_vectorised_layout_matches_pair_loop():
         blk = lay.rot[i] @ D[np.ix_(lay.atom_aos[i], lay.atom_aos[j])] @ lay.rot[j].T
         assert np.allclose(T[p, :blk.size], blk.ravel(), atol=1e-5 * np.max(np.abs(D)))
         assert M[p, :blk.size].all() and not M[p, blk.size:].any()
+
+
+def test_sad_atom_ao_indices_follow_the_reference_order():
+    """Per-atom AO indices of the SAD guess: the reference order (angular
+    momentum, component, atom, shell), checked against a direct enumeration."""
+    from veloxchem_b200 import MolecularBasis
+    from veloxchem_b200.geometry import water_cluster
+    from veloxchem_b200.scf import SadGuessDriver
+    mol = water_cluster((2, 1, 1), 5)
+    for name in ('def2-tzvp', 'ao-start-guess'):
+        bas = MolecularBasis.read(mol, name)
+        expect = [[] for _ in range(mol.number_of_atoms())]
+        ao = 0
+        for l in range(bas.max_angular_momentum() + 1):
+            for _m in range(2 * l + 1):
+                for a in range(mol.number_of_atoms()):
+                    for s in bas.shells:
+                        if s.atom == a and s.l == l:
+                            expect[a].append(ao)
+                            ao += 1
+        assert SadGuessDriver.ao_indices_of_atoms(mol, bas) == expect
+        assert ao == bas.get_dimensions_of_basis()

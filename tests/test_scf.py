@@ -136,3 +136,20 @@ def test_incremental_fock_builds_reach_the_full_build_energy():
     assert abs(res[True]['scf_energy'] - res[False]['scf_energy']) < 1e-9
     assert any(h.get('incremental') for h in res[True]['history'])
     assert not res[True]['history'][-1].get('incremental')
+
+
+@pytest.mark.gpu
+def test_early_loose_iterations_reach_the_reference_energy():
+    """Early iterations at ithreshold 8 with FP32 below 1e-4 (mixed precision,
+    incremental builds): the converged energy is still the reference's, and
+    the early iterations did use the looser threshold."""
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol, bas = _dimer()
+    drv = ScfRestrictedDriver()
+    drv.fp32_cutoff = 1e-6
+    drv.early_ithreshold = 8
+    res = drv.compute(mol, bas)
+    assert res['converged']
+    assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
+    assert res['history'][0]['ithreshold'] == 8
+    assert res['history'][-1]['ithreshold'] == 12

@@ -47,8 +47,9 @@ struct OneShellSet {
     const double* coefs;
     int nshells;
 };
-void launch_one_electron(int which, const OneShellSet& bra, const OneShellSet& ket, int natoms, const double* zc,
-                         const double* cxyz, const double* boys, double* out, int nao_ket, cudaStream_t st);
+void launch_one_electron(int which, const OneShellSet& bra, const OneShellSet& ket, int sym, int natoms,
+                         const double* zc, const double* cxyz, const double* boys, double* out, int nao_ket,
+                         cudaStream_t st);
 }  // namespace vlx
 
 using vlx::FockArgs;
@@ -1339,7 +1340,10 @@ int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const
     }
     if (!rc) {
         cudaMemset(dout, 0, obytes);
-        vlx::launch_one_electron(which, sets[0], sets[1], natoms, static_cast<const double*>(dz),
+        // the same basis on both sides: S, T, V are symmetric, one triangle of shell pairs is evaluated
+        const bool sym = hb.l == hk.l && hb.nprim == hk.nprim && hb.xyz == hk.xyz && hb.exps == hk.exps &&
+                         hb.coefs == hk.coefs;
+        vlx::launch_one_electron(which, sets[0], sets[1], sym ? 1 : 0, natoms, static_cast<const double*>(dz),
                                  static_cast<const double*>(dxyz), g->boys, static_cast<double*>(dout), hk.nao, 0);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(out, dout, obytes, cudaMemcpyDeviceToHost);

@@ -99,13 +99,26 @@ __device__ void hermite_e(const int la, const int lbmax, const double p, const d
     }
 }
 
-__global__ void one_electron_kernel(const int which, const OneShellSet bra, const OneShellSet ket, const int natoms,
-                                    const double* __restrict__ zc, const double* __restrict__ cxyz,
+// sym: bra and ket are the same basis; thread pid takes the pair sa <= sb of
+// the packed upper triangle and writes the block and its transpose.
+__global__ void one_electron_kernel(const int which, const OneShellSet bra, const OneShellSet ket, const int sym,
+                                    const int natoms, const double* __restrict__ zc, const double* __restrict__ cxyz,
                                     const double* __restrict__ boys, double* __restrict__ out, const int nao_ket)
 {
     const long long pid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pid >= (long long)bra.nshells * ket.nshells) return;
-    const int sa = (int)(pid / ket.nshells), sb = (int)(pid % ket.nshells);
+    int sa, sb;
+    if (sym) {
+        if (pid >= (long long)bra.nshells * (bra.nshells + 1) / 2) return;
+        long long t = (long long)((sqrt(8.0 * (double)pid + 1.0) - 1.0) * 0.5);
+        while (t * (t + 1) / 2 > pid) t--;
+        while ((t + 1) * (t + 2) / 2 <= pid) t++;
+        sb = (int)t;
+        sa = (int)(pid - t * (t + 1) / 2);
+    } else {
+        if (pid >= (long long)bra.nshells * ket.nshells) return;
+        sa = (int)(pid / ket.nshells);
+        sb = (int)(pid % ket.nshells);
+    }
     const int la = bra.l[sa], lb = ket.l[sb];
     const double A[3] = {bra.xyz[3 * sa], bra.xyz[3 * sa + 1], bra.xyz[3 * sa + 2]};
     const double B[3] = {ket.xyz[3 * sb], ket.xyz[3 * sb + 1], ket.xyz[3 * sb + 2]};
@@ -123,9 +136,14 @@ __global__ void one_electron_kernel(const int which, const OneShellSet bra, cons
             for (int d = 0; d < 3; d++) {
                 P[d] = (a * A[d] + b * B[d]) / p;
                 ab2 += (A[d] - B[d]) * (A[d] - B[d]);
-                hermite_e(la, lbmax, p, P[d] - A[d], P[d] - B[d], E[d]);
             }
             const double kab = ca * cb * exp(-mu * ab2);
+            // a primitive pair whose Gaussian-product prefactor is below 1e-40
+            // contributes below 1e-20 to any of S, T, V (the Hermite factors,
+            // (pi/p)^(3/2), b^2 and the nuclear charges stay far below 1e20
+            // for molecular distances)
+            if (fabs(kab) < 1.0e-40) continue;
+            for (int d = 0; d < 3; d++) hermite_e(la, lbmax, p, P[d] - A[d], P[d] - B[d], E[d]);
             if (which <= 1) {
                 const double s1 = sqrt(M_PI / p);  // 1D overlap factor
                 for (int ia = 0; ia < nca; ia++) {
@@ -210,16 +228,18 @@ __global__ void one_electron_kernel(const int which, const OneShellSet bra, cons
             }
             const size_t row = bra.ao0[sa] + i * bra.nl[la], col = ket.ao0[sb] + j * ket.nl[lb];
             out[row * nao_ket + col] = v;
+            if (sym && sa != sb) out[col * nao_ket + row] = v;
         }
 }
 
-void launch_one_electron(int which, const OneShellSet& bra, const OneShellSet& ket, int natoms, const double* zc,
-                         const double* cxyz, const double* boys, double* out, int nao_ket, cudaStream_t st)
+void launch_one_electron(int which, const OneShellSet& bra, const OneShellSet& ket, int sym, int natoms,
+                         const double* zc, const double* cxyz, const double* boys, double* out, int nao_ket,
+                         cudaStream_t st)
 {
-    const long long n = (long long)bra.nshells * ket.nshells;
+    const long long n = sym ? (long long)bra.nshells * (bra.nshells + 1) / 2 : (long long)bra.nshells * ket.nshells;
     const int threads = 64;
-    one_electron_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(which, bra, ket, natoms, zc, cxyz,
-                                                                                    boys, out, nao_ket);
+    one_electron_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(which, bra, ket, sym, natoms, zc,
+                                                                                    cxyz, boys, out, nao_ket);
 }
 
 }  // namespace vlx

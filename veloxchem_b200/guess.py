@@ -281,7 +281,8 @@ class LearnedGuessDriver:
         svp = MolecularBasis.read(molecule, 'def2-svp')
         minb = MolecularBasis.read(molecule, 'ao-start-guess')
         s_svp = nat.one_electron(0, molecule, svp, None, self.device)
-        d_svp = self.predict(molecule, svp, SadGuessDriver().compute(molecule, minb, svp, self.device), s_svp, nocc)
+        d_sad = SadGuessDriver().compute(molecule, minb, svp, self.device, overlap=s_svp)
+        d_svp = self.predict(molecule, svp, d_sad, s_svp, nocc)
         if basis.name.upper() == 'DEF2-SVP':
             return d_svp
         if refine_grad:

@@ -68,21 +68,26 @@ class SadGuessDriver:
 
     @staticmethod
     def ao_indices_of_atoms(molecule, basis):
+        """AO indices of each atom's functions in the reference AO order
+        (angular momentum, then component m, then atom, then shell)."""
         natoms = molecule.number_of_atoms()
+        shells_of = {}  # (l, atom) -> number of shells
+        for s in basis.shells:
+            shells_of[(s.l, s.atom)] = shells_of.get((s.l, s.atom), 0) + 1
         idx = [[] for _ in range(natoms)]
         ao = 0
         for l in range(basis.max_angular_momentum() + 1):
             for _m in range(2 * l + 1):
                 for a in range(natoms):
-                    for s in basis.shells:
-                        if s.atom == a and s.l == l:
-                            idx[a].append(ao)
-                            ao += 1
+                    n = shells_of.get((l, a), 0)
+                    idx[a].extend(range(ao, ao + n))
+                    ao += n
         return idx
 
-    def compute(self, molecule, min_basis, ao_basis, device=0):
+    def compute(self, molecule, min_basis, ao_basis, device=0, overlap=None):
+        """overlap: the AO-basis overlap matrix if the caller has it already."""
         s12 = nat.one_electron(0, molecule, min_basis, ao_basis, device)
-        s22 = nat.one_electron(0, molecule, ao_basis, None, device)
+        s22 = nat.one_electron(0, molecule, ao_basis, None, device) if overlap is None else np.asarray(overlap)
         ao1 = self.ao_indices_of_atoms(molecule, min_basis)
         ao2 = self.ao_indices_of_atoms(molecule, ao_basis)
         csad = np.zeros((s22.shape[0], s12.shape[0]))
@@ -121,6 +126,16 @@ class ScfRestrictedDriver:
         # final iterations are FP64, so the converged energy is the FP64 one
         self.fp32_cutoff = 0.0
         self.fp32_until_grad = 1.0e-4
+        # early iterations (until the electronic gradient first drops to
+        # early_until_grad) built at the looser integral threshold
+        # 10^-early_ithreshold and, in mixed precision, with FP32 below
+        # early_fp32_cutoff; None keeps the reference's dynamic threshold
+        # throughout.  The switch is one-way; the first iteration after it is
+        # a full build (the threshold changed) and starts a new DIIS subspace
+        # (the early Fock matrices carry the looser threshold's error)
+        self.early_ithreshold = None
+        self.early_until_grad = 1.0e-2
+        self.early_fp32_cutoff = 1.0e-4
         # incremental Fock builds: F_n = F_(n-1) + G(D_n - D_(n-1)) with the
         # screening threshold tightened by max|D_n - D_(n-1)| (a quartet is
         # dropped when its Schwarz bound times max|dD| is below a hundredth of
@@ -144,6 +159,15 @@ class ScfRestrictedDriver:
             return self.eri_thresh
         return nteri
 
+    def _ithreshold(self, e_grad, early):
+        ith = int(-math.log10(self.dyn_threshold(e_grad)))
+        return min(ith, int(self.early_ithreshold)) if early else ith
+
+    def _fp32_cutoff(self, early):
+        if self.fp32_cutoff <= 0.0:
+            return 0.0
+        return max(self.fp32_cutoff, self.early_fp32_cutoff) if early else self.fp32_cutoff
+
     def compute(self, molecule, ao_basis, min_basis=None, guess_density=None, screener=None):
         torch = _torch()
         dev = torch.device('cuda', self.device)
@@ -153,7 +177,8 @@ class ScfRestrictedDriver:
             raise ValueError('ScfRestrictedDriver: odd number of electrons')
         nocc = nelec // 2
         t0 = time.perf_counter()
-        S = torch.from_numpy(nat.one_electron(0, molecule, ao_basis, None, self.device)).to(dev)
+        S_host = nat.one_electron(0, molecule, ao_basis, None, self.device)
+        S = torch.from_numpy(S_host).to(dev)
         T = torch.from_numpy(nat.one_electron(1, molecule, ao_basis, None, self.device)).to(dev)
         V = torch.from_numpy(nat.one_electron(2, molecule, ao_basis, None, self.device)).to(dev)
         H = T + V
@@ -174,7 +199,7 @@ class ScfRestrictedDriver:
         elif self.guess in ('sad', 'learned'):
             if min_basis is None:
                 min_basis = MolecularBasis.read(molecule, 'ao-start-guess')
-            D_sad = SadGuessDriver().compute(molecule, min_basis, ao_basis, self.device)
+            D_sad = SadGuessDriver().compute(molecule, min_basis, ao_basis, self.device, overlap=S_host)
             D = torch.from_numpy(D_sad).to(dev)
         else:
             e, c = torch.linalg.eigh(X.T @ H @ X)
@@ -200,7 +225,7 @@ class ScfRestrictedDriver:
             D_l = learned_guess_driver(self.guess_weights, self.device).predict_any(molecule, ao_basis,
                                                                                    S.cpu().numpy(), nocc, D_sad, X)
             self.timings['learned_guess_s'] = time.perf_counter() - t0
-            ith0 = int(-math.log10(self.dyn_threshold(1.0)))
+            ith0 = self._ithreshold(1.0, self.early_ithreshold is not None)
             # the learned candidate is built as iteration 1 would build it (its
             # F is reused there); the SAD candidate's energy only has to rank
             # the two guesses, whose energies differ by far more than the error
@@ -208,7 +233,8 @@ class ScfRestrictedDriver:
             dl = torch.from_numpy(D_l).to(dev)
             dl = 0.5 * (dl + dl.T).contiguous()
             fl = torch.empty_like(dl)
-            screener.set_fp32_threshold(self.fp32_cutoff, float(torch.max(torch.abs(dl))))
+            screener.set_fp32_threshold(self._fp32_cutoff(self.early_ithreshold is not None),
+                                        float(torch.max(torch.abs(dl))))
             build(dl, fl, ith0)
             ds = 0.5 * (D + D.T).contiguous()
             fs = torch.empty_like(ds)
@@ -241,10 +267,16 @@ class ScfRestrictedDriver:
             err = X.T @ (fds - fds.T) @ X
             return float(e_ee + e_one) + e_nuc, F, err, 2.0 * float(torch.linalg.norm(err))
 
+        early = self.early_ithreshold is not None
         for it in range(1, self.max_iter + 1):
-            ith = int(-math.log10(self.dyn_threshold(e_grad)))
+            if early and e_grad <= self.early_until_grad:
+                early = False
+                focks.clear()
+                errs.clear()
+            ith = self._ithreshold(e_grad, early)
             D = 0.5 * (D + D.T).contiguous()
             mixed = self.fp32_cutoff > 0.0 and e_grad > self.fp32_until_grad
+            cutoff = self._fp32_cutoff(early) if mixed else 0.0
             inc = (incremental and first is None and D_prev is not None and ith == ith_prev
                    and since_full + 1 < self.rebuild_every)
             t0 = time.perf_counter()
@@ -256,12 +288,12 @@ class ScfRestrictedDriver:
                 dD = (D - D_prev).contiguous()
                 m = float(torch.max(torch.abs(dD)))
                 ith_used = min(ith, max(0, ith + 2 + math.floor(math.log10(m)))) if m > 0.0 else ith
-                screener.set_fp32_threshold(self.fp32_cutoff if mixed else 0.0, m)
+                screener.set_fp32_threshold(cutoff, m)
                 build(dD, G, ith_used)
                 F2e.copy_(F2e_prev)
                 F2e.add_(G)
             else:
-                screener.set_fp32_threshold(self.fp32_cutoff if mixed else 0.0, float(torch.max(torch.abs(D))))
+                screener.set_fp32_threshold(cutoff, float(torch.max(torch.abs(D))))
                 build(D, F2e, ith)
                 ith_used = ith
             torch.cuda.synchronize(dev)

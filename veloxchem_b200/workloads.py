@@ -89,25 +89,27 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=T
     if scf:
         runs = {}
         # plain: FP64 builds from the full density every iteration, SAD guess
-        for name, cut, guess, inc in (('plain_fp64_sad', 0.0, 'sad', False),
-                                      ('fp64_sad_incremental', 0.0, 'sad', True),
-                                      ('mixed_1e-6_sad', 1e-6, 'sad', False),
-                                      ('fp64_learned', 0.0, 'learned', False),
-                                      ('mixed_learned_incremental', 1e-6, 'learned', True)):
+        for name, cut, guess, inc, early in (('plain_fp64_sad', 0.0, 'sad', False, None),
+                                             ('fp64_sad_incremental', 0.0, 'sad', True, None),
+                                             ('mixed_1e-6_sad', 1e-6, 'sad', False, None),
+                                             ('fp64_learned', 0.0, 'learned', False, None),
+                                             ('mixed_learned_incremental', 1e-6, 'learned', True, None),
+                                             ('mixed_learned_incremental_early8', 1e-6, 'learned', True, 8)):
             if variants and name not in variants:
                 continue
             drv = ScfRestrictedDriver()
             drv.fp32_cutoff = cut
             drv.guess = guess
             drv.incremental = inc
+            drv.early_ithreshold = early
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
             runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
                           'converged': res['converged'], 'wall_s': time.perf_counter() - t0,
                           'fock_ms_total': res['timings']['fock_ms_total'], 'guess_used': res['guess_used'],
                           'timings': {k: v for k, v in res['timings'].items() if isinstance(v, float)},
-                          'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'])
-                                      for h in res['history']]}
+                          'history': [(h['iteration'], h['energy'], h['e_grad'], h['time_s'], h['mixed'],
+                                       h['ithreshold'], h['incremental']) for h in res['history']]}
         # E_ref: the plain FP64 run (or, if it was not run, the last variant's energy)
         e_ref = runs['plain_fp64_sad']['energy'] if 'plain_fp64_sad' in runs else list(runs.values())[-1]['energy']
         for r in runs.values():
