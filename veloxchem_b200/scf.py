@@ -304,7 +304,9 @@ class ScfRestrictedDriver:
                                  'ithreshold': ith_used, 'mixed': mixed, 'incremental': inc,
                                  'time_s': time.perf_counter() - t_start})
             e_old = energy
-            if e_grad < self.conv_thresh and inc:
+            # convergence is never declared on an early (looser-threshold)
+            # build: the next iteration switches back and rebuilds in full
+            if e_grad < self.conv_thresh and inc and not early:
                 # confirm on a full FP64 build of the same density
                 t0 = time.perf_counter()
                 screener.set_fp32_threshold(0.0, 0.0)
@@ -318,7 +320,7 @@ class ScfRestrictedDriver:
                                      'time_s': time.perf_counter() - t_start})
                 if e_grad >= self.conv_thresh:
                     incremental = False
-            if e_grad < self.conv_thresh:
+            if e_grad < self.conv_thresh and not early:
                 converged = True
                 break
             D_prev, F2e_prev, ith_prev = D, F2e.clone(), ith
