@@ -168,3 +168,4 @@ def test_sad_atom_ao_indices_follow_the_reference_order():
                             ao += 1
         assert SadGuessDriver.ao_indices_of_atoms(mol, bas) == expect
         assert ao == bas.get_dimensions_of_basis()
+

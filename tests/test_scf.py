@@ -153,3 +153,17 @@ def test_early_loose_iterations_reach_the_reference_energy():
     assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
     assert res['history'][0]['ithreshold'] == 8
     assert res['history'][-1]['ithreshold'] == 12
+
+
+def test_scf_threshold_schedule():
+    """The reference's dynamic ERI threshold (ScfDriver._get_dyn_threshold:
+    1e-10 for gradients >= 1, one decade tighter per decade of gradient, 1e-12
+    floor) and the optional looser early iterations."""
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    drv = ScfRestrictedDriver()
+    assert [drv._ithreshold(g, False) for g in (20.0, 1.0, 0.5, 0.05, 5e-3, 1e-7)] == [10, 10, 11, 12, 12, 12]
+    drv.early_ithreshold = 8
+    assert [drv._ithreshold(g, True) for g in (20.0, 0.5, 5e-3)] == [8, 8, 8]
+    assert drv._fp32_cutoff(True) == 0.0  # mixed precision off: no FP32 at all
+    drv.fp32_cutoff = 1e-6
+    assert drv._fp32_cutoff(True) == 1e-4 and drv._fp32_cutoff(False) == 1e-6
