@@ -184,18 +184,20 @@ def c2scf():
     from .scf import ScfRestrictedDriver
     mol, bas = _cluster('h2o32', 'def2-svp')
     runs = {}
-    for name, cut, inc in (('warmup', 0.0, False), ('plain_fp64', 0.0, False), ('mixed_1e-6', 1e-6, False),
-                           ('fp64_incremental', 0.0, True), ('mixed_incremental', 1e-6, True)):
+    for name, cut, inc, early in (('warmup', 0.0, False, None), ('plain_fp64', 0.0, False, None),
+                                  ('mixed_1e-6', 1e-6, False, None), ('fp64_incremental', 0.0, True, None),
+                                  ('mixed_incremental', 1e-6, True, None), ('mixed_incremental_early8', 1e-6, True, 8)):
         drv = ScfRestrictedDriver()
         drv.fp32_cutoff = cut
         drv.incremental = inc
+        drv.early_ithreshold = early
         t0 = time.perf_counter()
         res = drv.compute(mol, bas)
         if name == 'warmup':
             continue
         runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
                       'wall_s': time.perf_counter() - t0, 'fock_ms_total': res['timings']['fock_ms_total']}
-    for k in ('mixed_1e-6', 'fp64_incremental', 'mixed_incremental'):
+    for k in ('mixed_1e-6', 'fp64_incremental', 'mixed_incremental', 'mixed_incremental_early8'):
         runs[k]['energy_error'] = runs[k]['energy'] - runs['plain_fp64']['energy']
     return {'workload': '(H2O)32 / def2-SVP RHF from SAD, gradient < 1e-6', **runs}
 
