@@ -131,6 +131,27 @@ int vlx_b200_fock_build_device(vlx_b200_screener* screener, const double* d_dens
                                const char* label, double exchange_factor, double omega, int ithreshold,
                                double* d_fock, void* stream);
 
+/* Device-resident share of rank `rank` out of `nodes` (as
+ * vlx_b200_fock_build_local, with device pointers and a stream as in
+ * vlx_b200_fock_build_device); the partition of the work items is the one
+ * set by vlx_b200_set_partition.  The caller sums the shares (one all-reduce
+ * of the nao x nao FP64 partials).
+ * Replaces CFockDriver::compute(screener, rank, nodes, density, ...)
+ * (src/t4c_func/FockDriver.cpp:234-290) for a caller whose matrices live on
+ * the GPU. */
+int vlx_b200_fock_build_local_device(vlx_b200_screener* screener, int rank, int nodes, const double* d_density,
+                                     int symmetric, const char* label, double exchange_factor, double omega,
+                                     int ithreshold, double* d_fock, void* stream);
+
+/* Partition of the work items over ranks for the rank/nodes builds of this
+ * screener: 0 (default) deals them round-robin, as the reference's
+ * omp::partition_tasks (src/general/OpenMPFunc.hpp:89-112) does, so a rank's
+ * share equals the reference's; 1 assigns each item to the rank with the
+ * least estimated work so far (greedy list scheduling over the items'
+ * algorithmic flops), which balances ranks whose round-robin shares differ.
+ * The sum over ranks is the full build in both modes. */
+int vlx_b200_set_partition(vlx_b200_screener* screener, int mode);
+
 /* Largest basis accepted by vlx_b200_fock_build_noalloc. */
 #define VLX_B200_NOALLOC_MAX_NAO 1024
 
@@ -154,6 +175,8 @@ int vlx_b200_fock_build_device(vlx_b200_screener* screener, const double* d_dens
  *  - the screener must already hold the work list of `ithreshold`: one
  *    ordinary build (vlx_b200_fock_build*) with that threshold creates it;
  *    otherwise VLX_B200_ERR_ARGUMENT;
+ *  - the screener's mixed-precision split (vlx_b200_set_fp32_threshold)
+ *    applies as in vlx_b200_fock_build_device;
  *  - the first call on a device looks up the address of the static array on
  *    that device, so make that first call before any stream capture;
  *  - all calls share the one array, which keeps the previous call's contents

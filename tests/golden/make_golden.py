@@ -11,10 +11,11 @@ checkout and the compiled reference oracle are available).
   seeded random density, and J, K, 2J-K at ithreshold 12 from the reference
   FockDriver compiled from source (oracle/_ref/libvlxref.so).
 
-    python tests/golden/make_golden.py /path/to/reference
+    python tests/golden/make_golden.py [/path/to/reference]   (default: $VLX_REFERENCE_DIR)
 """
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -49,8 +50,18 @@ def _geom(text):
     return np.array(ids, dtype=np.int32), np.array(xyz)
 
 
+def reference_dir():
+    """The reference checkout: $VLX_REFERENCE_DIR, else a directory named
+    ``reference`` next to this repository."""
+    env = os.environ.get('VLX_REFERENCE_DIR')
+    ref = Path(env) if env else HERE.parents[2] / 'reference'
+    if not (ref / 'tests' / 'data').is_dir():
+        raise SystemExit('reference checkout not found at %s: set VLX_REFERENCE_DIR' % ref)
+    return ref
+
+
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else reference_dir()
     data = ref / 'tests' / 'data'
 
     z, xyz = _geom(H2O)

@@ -69,3 +69,28 @@ def test_noalloc_needs_existing_work_list():
     f = torch.zeros_like(d)
     assert _noalloc(scr, d, f, ith=11) == 1
     assert b'work list' in nat.lib().vlx_b200_last_error()
+
+
+def test_noalloc_honours_mixed_precision():
+    """With the screener's FP32 split active the allocation-free build
+    evaluates the same quartets in FP32 as the allocating device build."""
+    import ctypes
+    import torch
+    from veloxchem_b200 import _native as nat
+    mol, bas, scr, dens = _system((2, 2, 2), 8, 3)
+    d = torch.from_numpy(dens).cuda()
+    f64, fmix, fna = torch.zeros_like(d), torch.zeros_like(d), torch.zeros_like(d)
+
+    def device_build(out):
+        nat.check(nat.lib().vlx_b200_fock_build_device(scr.handle, ctypes.c_void_p(d.data_ptr()), 1, b'2jk', 1.0,
+                                                        0.0, 12, ctypes.c_void_p(out.data_ptr()), None),
+                  'fock_build_device')
+
+    device_build(f64)
+    scr.set_fp32_threshold(1e-3, float(d.abs().max()))
+    device_build(fmix)
+    nat.check(_noalloc(scr, d, fna), 'fock_build_noalloc')
+    torch.cuda.synchronize()
+    scr.set_fp32_threshold(0.0, 0.0)
+    assert float((fmix - f64).abs().max()) > 1e-10      # the FP32 quartets changed the matrix
+    assert float((fna - fmix).abs().max()) < 1e-10      # ... and the same way in both builds

@@ -39,6 +39,10 @@ SIGNATURES = {
                                                  ctypes.c_int, ctypes.POINTER(_dp), _vp]),
     'vlx_b200_fock_build_device': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
                                                   ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    'vlx_b200_fock_build_local_device': (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                        ctypes.c_char_p, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_int, _vp, _vp]),
+    'vlx_b200_set_partition': (ctypes.c_int, [_vp, ctypes.c_int]),
     'vlx_b200_compute_eri': (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     'vlx_b200_boys_device': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     'vlx_b200_fock_profile': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double, ctypes.c_int,

@@ -13,6 +13,7 @@ Usage (in a checkout that has the reference):
 """
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -52,8 +53,18 @@ def parse_basis_file(path):
     return atoms
 
 
+def reference_dir():
+    """The reference checkout: $VLX_REFERENCE_DIR, else a directory named
+    ``reference`` next to this repository."""
+    env = os.environ.get('VLX_REFERENCE_DIR')
+    ref = Path(env) if env else Path(__file__).resolve().parents[3] / 'reference'
+    if not (ref / 'basis').is_dir():
+        raise SystemExit('reference checkout not found at %s: set VLX_REFERENCE_DIR' % ref)
+    return ref
+
+
 def main():
-    src = Path(sys.argv[1] if len(sys.argv) > 1 else '/root/reference/basis')
+    src = Path(sys.argv[1]) if len(sys.argv) > 1 else reference_dir() / 'basis'
     out = Path(__file__).parent
     for name in BASIS_SETS:
         atoms = parse_basis_file(src / name)

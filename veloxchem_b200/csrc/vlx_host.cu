@@ -309,6 +309,7 @@ struct ClassTasks {
 
 struct TaskSet {
     int ith = 0, rank = 0, nodes = 1, seg = 0, tune_gen = 0;  // ith: the threshold the items were built for
+    int part = 0;  // partition of the items over nodes: 0 round-robin, 1 cost-balanced
     std::vector<ClassTasks> classes;
     WorkItem* d_items = nullptr;
     long long quartets = 0, prim_quartets = 0;
@@ -344,6 +345,7 @@ struct vlx_b200_screener {
     int seg_try_compiled = 0, seg_try_coop = 0;  // candidate lengths while tuning (0: off)
     int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
     int ith_base = -1;  // work lists are built for max(ithreshold, ith_base) and filtered at run time
+    int part = 0;       // rank/nodes partition of later builds: 0 round-robin (reference), 1 cost-balanced
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -521,11 +523,15 @@ int run_schwarz(vlx_b200_screener* s, std::vector<std::vector<double>>& maxv)
     return VLX_B200_OK;
 }
 
+double class_flops(const vlx_b200_screener* s, const ClassTasks& ct, long long quartets, long long prim_quartets);
+
 int build_tasks(vlx_b200_screener* s, int ith_req, int rank, int nodes, TaskSet** out)
 {
     const int ith = std::max(ith_req, s->ith_base);
+    const int part = (nodes > 1) ? s->part : 0;
     for (auto& t : s->tasksets)
-        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg && t.tune_gen == s->tune_gen) {
+        if (t.ith == ith && t.rank == rank && t.nodes == nodes && t.seg == s->seg && t.tune_gen == s->tune_gen &&
+            t.part == part) {
             *out = &t;
             return VLX_B200_OK;
         }
@@ -533,6 +539,11 @@ int build_tasks(vlx_b200_screener* s, int ith_req, int rank, int nodes, TaskSet*
     ts.ith = ith;
     ts.rank = rank;
     ts.nodes = nodes;
+    ts.part = part;
+    // cost-balanced partition: every rank deals the same item sequence, each
+    // item to the rank with the least estimated work so far (greedy list
+    // scheduling over the algorithmic flops of the item)
+    std::vector<double> load(part ? nodes : 0, 0.0);
     ts.seg = s->seg;
     ts.tune_gen = s->tune_gen;
     std::map<int, int> cls_index;  // key -> position in ts.classes
@@ -583,7 +594,16 @@ int build_tasks(vlx_b200_screener* s, int ith_req, int rank, int nodes, TaskSet*
                 }
                 for (int k0 = kbeg; k0 < kend; k0 += seg) {
                     const int k1 = std::min(kend, k0 + seg);
-                    if ((g++ % nodes) != rank) continue;
+                    if (part) {
+                        const long long prim = (long long)Pb.nuse[x] * (Pk.nuse_prefix[k1] - Pk.nuse_prefix[k0]);
+                        int owner = 0;
+                        for (int r = 1; r < nodes; r++)
+                            if (load[r] < load[owner]) owner = r;
+                        load[owner] += class_flops(s, ct, k1 - k0, prim);
+                        if (owner != rank) continue;
+                    } else if ((g++ % nodes) != rank) {
+                        continue;
+                    }
                     WorkItem w;
                     w.blocks = (int)bra | ((int)ket << 16);
                     w.bra = x;
@@ -1129,6 +1149,25 @@ int vlx_b200_fock_build_device(vlx_b200_screener* s, const double* d_density, in
     return device_build(s, 0, 1, d_density, symmetric, label, xfac, omega, ith, d_fock, st, nullptr, nullptr, nullptr);
 }
 
+int vlx_b200_fock_build_local_device(vlx_b200_screener* s, int rank, int nodes, const double* d_density,
+                                     int symmetric, const char* label, double xfac, double omega, int ith,
+                                     double* d_fock, void* stream)
+{
+    if (!s || !d_density || !d_fock) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
+    VLX_CUDA(cudaSetDevice(s->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    return device_build(s, rank, nodes, d_density, symmetric, label, xfac, omega, ith, d_fock, st, nullptr, nullptr,
+                        nullptr);
+}
+
+int vlx_b200_set_partition(vlx_b200_screener* s, int mode)
+{
+    if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
+    if (mode != 0 && mode != 1) return fail(VLX_B200_ERR_ARGUMENT, "set_partition: mode must be 0 or 1");
+    s->part = mode;
+    return VLX_B200_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ allocation-free build
@@ -1141,7 +1180,7 @@ namespace {
 
 constexpr int kNoallocMaxClasses = 64;
 static __device__ __align__(256) double g_noalloc_acc[(size_t)VLX_B200_NOALLOC_MAX_NAO * VLX_B200_NOALLOC_MAX_NAO];
-static __device__ __align__(256) int g_noalloc_heads[kNoallocMaxClasses];
+static __device__ __align__(256) int g_noalloc_heads[2 * kNoallocMaxClasses];  // FP64, then FP32 heads
 
 struct NoallocScratch {
     double* acc = nullptr;
@@ -1201,44 +1240,23 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
     if (rc) return rc;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
-    // the arrays keep the previous call's contents: clear the accumulator and the queue heads
+    // the arrays keep the previous call's contents: clear the accumulator here
+    // (the class launches clear their own queue heads, FP64 and FP32 blocks)
     VLX_CUDA(cudaMemsetAsync(sc.acc, 0, bytes, st));
     if (known && !ts->classes.empty()) {
-        VLX_CUDA(cudaMemsetAsync(sc.heads, 0, ts->classes.size() * sizeof(int), st));
-        FockArgs a;
-        std::memset(&a, 0, sizeof(a));
-        a.blocks = s->d_blocks;
-        a.boys = s->glob->boys;
-        a.mol.D = d_density;
-        a.mol.F = sc.acc;
-        a.mol.nao = s->nao;
-        for (int l = 0; l <= VLX_LMAX; l++) a.mol.nl[l] = s->nl[l];
-        a.cj = cj;
-        a.ck = ck;
-        a.omega2 = rs ? omega * omega : 0.0;
-        a.ith = ith;
-        a.ith32 = -1;
-        const int mode = symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN;
-        for (size_t c = 0; c < ts->classes.size(); c++) {
-            const ClassTasks& ct = ts->classes[c];
-            if (ct.items.empty()) continue;
-            a.items = ts->d_items + ct.offset;
-            a.nitems = (int)ct.items.size();
-            a.counter = sc.heads + c;
-            if (ct.compiled >= 0) {
-                const auto& e = vlx::kQuartetClasses[ct.compiled];
-                const int want = (int)((ct.items.size() + vlx::kWarpsPerBlock - 1) / vlx::kWarpsPerBlock);
-                const int grid = std::max(1, std::min(want, std::max(1, e.occupancy(mode)) * s->glob->nsm));
-                e.launch(mode, a, grid, st);
-            } else {
-                const CoopClassDev& cc = s->glob->coop[ct.coop];
-                const int wpb = vlx::coop_warps_per_block(cc);
-                const int cap = vlx::coop_blocks_per_sm(cc) * s->glob->nsm;
-                const int grid = std::max(1, std::min((int)((ct.items.size() + wpb - 1) / wpb), cap));
-                VLX_CUDA(vlx::launch_coop_quartet(mode, a, cc, grid, st));
-            }
-            VLX_CUDA(cudaGetLastError());
-        }
+        LaunchCtx L;
+        L.blocks = s->d_blocks;
+        L.glob = s->glob;
+        L.counters = sc.heads;
+        L.mol.D = d_density;
+        L.mol.F = sc.acc;
+        L.mol.nao = s->nao;
+        for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
+        // the screener's mixed-precision split (set_fp32_threshold) applies as
+        // in the allocating builds
+        rc = enqueue_ctx(L, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, nullptr, cj, ck,
+                         rs ? omega * omega : 0.0, ith, s->ith32, st, nullptr);
+        if (rc) return rc;
     }
     if (symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
@@ -1572,6 +1590,8 @@ struct vlx_b200_batch {
 
 namespace {
 
+void batch_release_graph(vlx_b200_batch* b);
+
 int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
 {
     for (auto& t : b->merged)
@@ -1632,7 +1652,13 @@ int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
         VLX_CUDA(cudaMemcpy(m.d_items, all.data(), total * sizeof(WorkItem), cudaMemcpyHostToDevice));
     }
     if (2 * (int)m.classes.size() > b->ncounters) {
-        if (b->d_counters) cudaFree(b->d_counters);
+        // the instantiated graph of an earlier threshold launches with the old
+        // queue heads: drop it with them (it is re-captured on its next use)
+        if (b->d_counters) {
+            VLX_CUDA(cudaDeviceSynchronize());
+            cudaFree(b->d_counters);
+        }
+        batch_release_graph(b);
         b->ncounters = std::max<int>(128, 2 * (int)m.classes.size());
         VLX_CUDA(cudaMalloc(&b->d_counters, b->ncounters * sizeof(int)));
     }

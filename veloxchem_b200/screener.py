@@ -118,6 +118,14 @@ class T4CScreener:
         run time, so builds at several thresholds share one list."""
         nat.check(nat.lib().vlx_b200_set_work_threshold(self.handle, int(ithreshold_base)), 'set_work_threshold')
 
+    def set_partition(self, partition):
+        """Work-item partition of the rank/nodes builds: 'round_robin' (the
+        reference's deal) or 'balanced' (greedy by estimated cost)."""
+        from .distributed import PARTITIONS
+        if partition not in PARTITIONS:
+            raise ValueError('T4CScreener.set_partition: unknown partition %r' % (partition,))
+        nat.check(nat.lib().vlx_b200_set_partition(self.handle, PARTITIONS[partition]), 'set_partition')
+
     def set_block_size_factor(self, factor):
         nat.check(nat.lib().vlx_b200_set_block_size_factor(self.handle, int(factor)), 'set_block_size_factor')
 

@@ -220,6 +220,112 @@ def build(cluster, basis, repeat=1, fp32_cutoff=0.0):
             'fp32_cutoff': fp32_cutoff}
 
 
+def _time_to(history, e_ref, tol=1e-6):
+    """Wall time (s) after which every later iteration's energy stays within
+    tol of e_ref, from an SCF history (None if it never does)."""
+    for k, h in enumerate(history):
+        if all(abs(x['energy'] - e_ref) < tol for x in history[k:]):
+            return h['time_s']
+    return None
+
+
+def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf=True, log=None):
+    """The north-star comparison on (H2O)64 / def2-TZVP in one process:
+
+    * builds: the plain FP64 2J-K build (device ms, CUDA events, best of 2
+      after one warm-up), then the mixed-precision build at each cutoff (one
+      timed build each, FP32 share, max |F_mixed - F_FP64|); the chosen cutoff
+      is the fastest one whose Fock error stays within ``max_fock_error``;
+    * SCF: plain (FP64 full builds every iteration, SAD guess, run to an
+      electronic gradient of 1e-8 so that its final energy E_ref is the FP64
+      reference) against mixed + learned + incremental + early iterations
+      (gradient 1e-6), back to back on one screener; per run the wall time to
+      |E - E_ref| < 1e-6 Eh for good, the time to its declared convergence,
+      iterations and the final energy error."""
+    from . import T4CScreener
+    from . import _native as nat
+    from .geometry import random_density
+    from .scf import ScfRestrictedDriver
+    torch = _torch()
+    say = log or (lambda *a: None)
+    mol, bas = _cluster('h2o64', 'def2-tzvp')
+    t0 = time.perf_counter()
+    scr = T4CScreener()
+    scr.partition(bas, mol, 'eri')
+    out = {'workload': '(H2O)64 / def2-TZVP, 2J-K, ithreshold 12', 'nao': scr.nao,
+           'screener_s': time.perf_counter() - t0}
+    d = torch.from_numpy(random_density(scr.nao, 320, 1)).cuda()
+    f64 = torch.empty_like(d)
+    t64 = _build_ms(scr, d, f64, reps=2)
+    prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
+    flops = sum(p['flops'] for p in prof)
+    out['fp64_build_ms'] = t64
+    out['fp64_tflops'] = flops / t64 / 1e9
+    say('c3 fp64 build %.1f ms' % t64)
+    dmax = float(d.abs().max())
+    sweep = []
+    for cut in cutoffs:
+        scr.set_fp32_threshold(cut, dmax)
+        fm = torch.empty_like(d)
+        tm = _build_ms(scr, d, fm, reps=0)
+        prof = nat.fock_profile(scr, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
+        n32 = sum(p['fp32_quartets'] for p in prof)
+        nq = sum(p['shell_quartets'] for p in prof)
+        sweep.append({'cutoff': cut, 'build_ms': tm, 'speedup': t64 / tm, 'fp32_share': n32 / max(nq, 1),
+                      'max_abs_fock_error': float((fm - f64).abs().max())})
+        say('c3 mixed %.0e: %.1f ms, err %.2e' % (cut, tm, sweep[-1]['max_abs_fock_error']))
+    scr.set_fp32_threshold(0.0, 0.0)
+    ok = [s for s in sweep if s['max_abs_fock_error'] <= max_fock_error] or sweep[:1]
+    best = min(ok, key=lambda s: s['build_ms'])
+    out['mixed_sweep'] = sweep
+    out['mixed_chosen'] = best
+    if scf:
+        runs = {}
+        for name, cut, guess, inc, early, conv in (('plain_fp64_sad', 0.0, 'sad', False, None, 1e-8),
+                                                  ('mixed_learned_incremental_early', best['cutoff'], 'learned',
+                                                   True, 8, 1e-6)):
+            drv = ScfRestrictedDriver()
+            drv.fp32_cutoff = cut
+            drv.guess = guess
+            drv.incremental = inc
+            drv.early_ithreshold = early
+            drv.conv_thresh = conv
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = drv.compute(mol, bas, screener=scr)
+            wall = time.perf_counter() - t0
+            hist = [h for h in res['history']]
+            t_conv6 = next((h['time_s'] for h in hist if h['e_grad'] < 1e-6 and not h.get('mixed')), None)
+            runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'], 'converged': res['converged'],
+                          'conv_thresh': conv, 'wall_s': wall, 'fock_s': res['timings']['fock_ms_total'] / 1e3,
+                          'time_to_grad_1e-6_s': t_conv6, 'guess_used': res['guess_used'], '_history': hist}
+            say('c3 scf %s: %d it, %.1f s' % (name, res['iterations'], wall))
+        e_ref = runs['plain_fp64_sad']['energy']
+        for r in runs.values():
+            hist = r.pop('_history')
+            r['energy_error'] = r['energy'] - e_ref
+            r['time_to_1e-6_Eh_s'] = _time_to(hist, e_ref)
+        out['scf'] = runs
+        out['scf_reference_energy'] = e_ref
+        p, m = runs['plain_fp64_sad'], runs['mixed_learned_incremental_early']
+        out['scf_speedup_time_to_1e-6_Eh'] = ((p['time_to_1e-6_Eh_s'] / m['time_to_1e-6_Eh_s'])
+                                              if p['time_to_1e-6_Eh_s'] and m['time_to_1e-6_Eh_s'] else None)
+        out['scf_speedup_to_declared_convergence'] = (p['time_to_grad_1e-6_s'] / m['wall_s']
+                                                      if p['time_to_grad_1e-6_s'] else None)
+    return out
+
+
+def c4_headline(count=256, nmax=16, reps=3):
+    """Batched builds/s of the 256-cluster workload (graph replay) and the
+    one-molecule-per-call rate, device time."""
+    r = c4(count, nmax, reps)
+    return {'workload': r['workload'], 'nao_total': r['nao_total'],
+            'batched_builds_per_s': r['batched_graph']['builds_per_s'],
+            'batched_ms': r['batched_graph']['ms_per_batch'],
+            'one_per_call_builds_per_s': r['one_per_call']['builds_per_s'],
+            'max_abs_error_vs_single': r['max_abs_error_vs_single']}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build'])
