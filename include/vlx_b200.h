@@ -186,7 +186,8 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_den
                                 const char* label, double exchange_factor, double omega, int ithreshold,
                                 double* d_fock, void* stream);
 
-/* Mixed precision for the following builds of this screener: shell quartets
+/* Mixed precision on the decade bins for the following builds of this
+ * screener (and per-quartet density screening off): shell quartets
  * whose Schwarz bound sqrt((ab|ab)) sqrt((cd|cd)) times max_abs_density is
  * below `cutoff` (decided on the decade bins: bound <= 10^-(bin_ab + bin_cd))
  * are evaluated with the FP32 recursion; digestion and the Fock accumulator
@@ -194,6 +195,26 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_den
  * an FP32 twin).  cutoff <= 0 switches it off (the default).  No counterpart in the
  * reference (its Fock build is FP64 throughout). */
 int vlx_b200_set_fp32_threshold(vlx_b200_screener* screener, double cutoff, double max_abs_density);
+
+/* Per-quartet density screening for the following builds of this screener
+ * (it replaces the decade-bin split of vlx_b200_set_fp32_threshold, which it
+ * switches off, as that call switches this one off).  Each build first takes
+ * the shell-block maxima d_AB = max |D_ab|, |D_ba| of its own density, then
+ * bounds every shell quartet continuously by
+ *     b = sqrt((PQ|PQ)) sqrt((RS|RS)) max(|c_J| max(d_PQ, d_RS),
+ *                                         |c_K| max(d_PR, d_PS, d_QR, d_QS))
+ * (c_J, c_K the weights of the label), the largest change one integral of
+ * the quartet can make to an element of F.  Quartets with b < skip_cutoff
+ * are not evaluated; those with b < fp32_cutoff are evaluated with the FP32
+ * recursion (FP64 digestion and accumulator); the rest in FP64.  Cutoffs
+ * <= 0 switch the part off; both 0 (the default) give the reference's
+ * screening alone (the Schwarz bins of ithreshold, independent of D).  The
+ * statistics of vlx_b200_fock_build count quartets before this screening;
+ * vlx_b200_fock_profile counts those evaluated.  Not available in
+ * vlx_b200_fock_build_noalloc (the maxima need device scratch) or in batched
+ * builds.  No counterpart in the reference (its Fock build screens on the
+ * Schwarz bins only, T4CScreener / BlockedGtoPairBlock). */
+int vlx_b200_set_density_screening(vlx_b200_screener* screener, double fp32_cutoff, double skip_cutoff);
 
 /* Dense (nao)^4 ERI tensor over the screened unique quartets (all eight
  * index permutations written), host buffer.

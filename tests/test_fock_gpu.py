@@ -261,6 +261,57 @@ def test_mixed_precision_build():
     assert float((f2 - f64).abs().max()) < 1e-12
 
 
+def test_density_screening_build():
+    """Per-quartet density screening (bound sqrt((PQ|PQ)(RS|RS)) x weighted
+    local shell-block maxima of |D|): both cutoffs 0 is the reference's
+    screening; an FP32 cutoff keeps every quartet, evaluates some in FP32 --
+    more than the decade-bin split at the same cutoff -- with the Fock error
+    below a tenth of the cutoff; a skip cutoff evaluates fewer quartets with
+    the error bounded; general densities are bounded in both orientations."""
+    import torch
+    from veloxchem_b200 import _native as nat
+    g, mol, bas = load_golden('h2o4_svp.npz')
+    s = _screener(mol, bas)
+    d = torch.from_numpy(g['density']).cuda()
+
+    def build(dens, symmetric=True):
+        f = torch.empty_like(dens)
+        prof = nat.fock_profile(s, dens.data_ptr(), f.data_ptr(), '2jk', 1.0, 12, symmetric)
+        return f, sum(p['shell_quartets'] for p in prof), sum(p['fp32_quartets'] for p in prof)
+
+    f64, nq, _ = build(d)
+    s.set_density_screening(0.0, 0.0)
+    f0, nq0, n320 = build(d)
+    assert nq0 == nq and n320 == 0 and float((f0 - f64).abs().max()) < 1e-13
+    dmax = float(d.abs().max())
+    for cutoff in (1e-9, 1e-7, 1e-5):
+        s.set_fp32_threshold(cutoff, dmax)
+        _, _, n32_bins = build(d)
+        s.set_density_screening(cutoff, 0.0)
+        fm, nqm, n32 = build(d)
+        err = float((fm - f64).abs().max())
+        print('density screening fp32 cutoff %.0e: FP32 %d of %d quartets (bins: %d), error %.2e'
+              % (cutoff, n32, nqm, n32_bins, err))
+        assert nqm == nq and n32 >= n32_bins and n32 > 0
+        assert err < 0.1 * cutoff
+    for skip in (1e-12, 1e-10):
+        s.set_density_screening(0.0, skip)
+        fs, nqs, _ = build(d)
+        err = float((fs - f64).abs().max())
+        print('density screening skip %.0e: %d of %d quartets, error %.2e' % (skip, nqs, nq, err))
+        assert nqs < nq
+        assert err < 1e4 * skip
+    # general (non-symmetric) density: the bound covers D_ab and D_ba
+    rng = np.random.default_rng(5)
+    dg = torch.from_numpy(g['density'] + 1e-3 * rng.standard_normal(g['density'].shape)).cuda()
+    s.set_density_screening(0.0, 0.0)
+    fg64, _, _ = build(dg, False)
+    s.set_density_screening(1e-7, 0.0)
+    fg, _, n32 = build(dg, False)
+    assert n32 > 0 and float((fg - fg64).abs().max()) < 1e-8
+    s.set_density_screening(0.0, 0.0)
+
+
 def test_mixed_precision_scf_energy():
     """SCF with FP32 small quartets until the gradient is below 1e-4 reaches the
     FP64 energy (the final iterations are FP64)."""

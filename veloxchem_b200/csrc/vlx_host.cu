@@ -249,6 +249,30 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
     }
 }
 
+// Shell-block maxima of |D| for per-quartet density screening: dsh[A nsh + B]
+// = max over the components a of shell A and b of shell B of |D_ab| and
+// |D_ba| (both orientations, so general densities are bounded too), rounded
+// up to float.  One thread per shell pair, B fastest.
+__global__ void shell_dmax_kernel(const double* __restrict__ D, const int nao, const int2* __restrict__ shinfo,
+                                  const int nsh, const int4 nl, float* __restrict__ dsh)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nsh * nsh) return;
+    const int A = (int)(idx / nsh), B = (int)(idx % nsh);
+    const int2 a = shinfo[A], b = shinfo[B];
+    const int sa = (a.y == 0) ? nl.x : (a.y == 1) ? nl.y : (a.y == 2) ? nl.z : nl.w;
+    const int sb = (b.y == 0) ? nl.x : (b.y == 1) ? nl.y : (b.y == 2) ? nl.z : nl.w;
+    double m = 0.0;
+    for (int i = 0; i < 2 * a.y + 1; i++) {
+        const size_t r = (size_t)(a.x + i * sa);
+        for (int j = 0; j < 2 * b.y + 1; j++) {
+            const size_t c = (size_t)(b.x + j * sb);
+            m = fmax(m, fmax(fabs(D[r * nao + c]), fabs(D[c * nao + r])));
+        }
+    }
+    dsh[idx] = __double2float_ru(m);
+}
+
 template <int M>
 __global__ void boys_test_kernel(const double* T, double* F, int n, const double* tab)
 {
@@ -346,6 +370,12 @@ struct vlx_b200_screener {
     int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
     int ith_base = -1;  // work lists are built for max(ithreshold, ith_base) and filtered at run time
     int part = 0;       // rank/nodes partition of later builds: 0 round-robin (reference), 1 cost-balanced
+    // per-quartet density screening of later builds (vlx_b200_set_density_screening; 0: off)
+    double dscr_fp32 = 0.0, dscr_skip = 0.0;
+    float* d_dsh = nullptr;      // nsh x nsh shell-block max |D| of the build's density
+    int2* d_shinfo = nullptr;    // per shell: AO index of component 0, angular momentum
+    unsigned long long* d_qstat = nullptr;  // profiled builds: [class][FP64, FP32][quartets, primitive quartets]
+    int nqstat = 0;
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -356,7 +386,7 @@ namespace {
 // arrays, 16-byte aligned).
 size_t fp32_offset(size_t n, size_t kp)
 {
-    const size_t bytes = (9 * kp * n + 3 * n) * sizeof(double) + (4 * n + 17) * sizeof(int);
+    const size_t bytes = (9 * kp * n + 3 * n) * sizeof(double) + (6 * n + 17) * sizeof(int);
     return (bytes + 15) & ~size_t(15);
 }
 
@@ -372,7 +402,7 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         const size_t n = sorted ? pb.sorted.size() : pb.pairs.size();
         npairs[b] = (int)n;
         const size_t k = (size_t)pb.ka * pb.kb;
-        size_t bytes = fp32_offset(n, k) + (9 * k * n + 3 * n) * sizeof(float);
+        size_t bytes = fp32_offset(n, k) + (9 * k * n + 4 * n) * sizeof(float);
         bytes = (bytes + 255) & ~size_t(255);
         offs[b + 1] = offs[b] + bytes;
     }
@@ -390,8 +420,10 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         int* nuse = ao + 2 * n;
         int* bins = nuse + n;     // Schwarz bin per pair (sorted order; 0 before screening)
         int* bin_off = bins + n;  // first pair of bin >= b (17 entries)
+        int* shl = bin_off + 17;  // shell index of A, then of B
         float* primf = reinterpret_cast<float*>(host.data() + offs[b] + fp32_offset(n, (size_t)kp));
         float* abf = primf + 9 * (size_t)kp * n;
+        float* qf = abf + 3 * n;  // Schwarz factor, rounded up (0 before screening)
         for (int k = 0; k <= 16; k++) bin_off[k] = sorted ? pb.bin_off[k] : 0;
         for (size_t i = 0; i < n; i++) {
             bins[i] = sorted ? pb.bin[pb.sorted[i]] : 0;
@@ -406,6 +438,9 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
             }
             ao[i] = A.ao0;
             ao[n + i] = B.ao0;
+            shl[i] = pb.pairs[ref].first;
+            shl[n + i] = pb.pairs[ref].second;
+            qf[i] = sorted ? std::nextafter((float)std::sqrt(pb.maxv[ref]), INFINITY) : 0.0f;
             std::vector<std::array<double, 9>> vals(kp);
             for (int ka = 0; ka < pb.ka; ka++)
                 for (int kb = 0; kb < pb.kb; kb++) {
@@ -460,6 +495,8 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
         d.nuse = d.ao + 2 * n;
         d.bin = d.nuse + n;
         d.bin_off = d.bin + n;
+        d.sh = d.bin_off + 17;
+        d.q = d.primf + (9 * (size_t)kp + 3) * n;
         d.npairs = (int)n;
         d.kprim = kp;
         d.la = pb.la;
@@ -693,6 +730,11 @@ struct LaunchCtx {
     int* counters = nullptr;
     vlx::MolDev mol{};
     const vlx::MolDev* mols = nullptr;
+    // per-quartet density screening (dsh != nullptr): FockArgs::dsh, tau_skip, tau32
+    const float* dsh = nullptr;
+    int nsh = 0;
+    float tau_skip = 0.0f, tau32 = 0.0f;
+    unsigned long long* qstat = nullptr;  // [class][FP64, FP32][2] quartet counters (profiled builds)
 };
 
 // Enqueues all class kernels of a task set on `st`; the accumulators must be
@@ -718,7 +760,12 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.ck = ck;
     a.omega2 = omega2;
     a.ith = std::min(ith, ts->ith);
-    a.ith32 = ith32;
+    a.ith32 = L.dsh ? -1 : ith32;
+    a.dsh = L.dsh;
+    a.nsh = L.nsh;
+    a.tau_skip = L.tau_skip;
+    a.tau32 = L.tau32;
+    const int nprec = (L.dsh ? L.tau32 > 0.0f : ith32 >= 0) ? 2 : 1;
     const int warps_per_block = vlx::kWarpsPerBlock;
     const int nsm = L.glob->nsm;
     for (size_t c = 0; c < ts->classes.size(); c++) {
@@ -727,9 +774,10 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
         a.items = ts->d_items + ct.offset;
         a.nitems = (int)ct.items.size();
         if (events) VLX_CUDA(cudaEventRecord((*events)[c].first, st));
-        for (int f = 0; f < (ith32 >= 0 ? 2 : 1); f++) {
+        for (int f = 0; f < nprec; f++) {
             FockArgs af = a;
             af.counter = L.counters + (f ? ts->classes.size() : 0) + c;
+            af.qstat = L.qstat ? L.qstat + (c * 2 + f) * 2 : nullptr;
             const int fmode = f ? (mode | vlx::MODE_F32) : mode;
             if (ct.compiled >= 0) {
                 const auto& e = vlx::kQuartetClasses[ct.compiled];
@@ -751,9 +799,30 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     return VLX_B200_OK;
 }
 
+bool dscr_active(const vlx_b200_screener* s) { return s->dscr_fp32 > 0.0 || s->dscr_skip > 0.0; }
+
+// Shell-block maxima of the build's density for per-quartet screening.
+int prepare_dscr(vlx_b200_screener* s, const double* dD, cudaStream_t st)
+{
+    const int nsh = (int)s->shells.size();
+    if (!s->d_dsh) {
+        VLX_CUDA(cudaMalloc(&s->d_dsh, (size_t)nsh * nsh * sizeof(float)));
+        std::vector<int2> info(nsh);
+        for (int i = 0; i < nsh; i++) info[i] = make_int2(s->shells[i].ao0, s->shells[i].l);
+        VLX_CUDA(cudaMalloc(&s->d_shinfo, nsh * sizeof(int2)));
+        VLX_CUDA(cudaMemcpy(s->d_shinfo, info.data(), nsh * sizeof(int2), cudaMemcpyHostToDevice));
+    }
+    const long long n = (long long)nsh * nsh;
+    const int4 nl = make_int4(s->nl[0], s->nl[1], s->nl[2], s->nl[3]);
+    shell_dmax_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dD, s->nao, s->d_shinfo, nsh, nl, s->d_dsh);
+    VLX_CUDA(cudaGetLastError());
+    return VLX_B200_OK;
+}
+
 int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
                     double cj, double ck, double omega2, int ith, int ith32, cudaStream_t st, long long* launches,
-                    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr)
+                    std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr,
+                    unsigned long long* qstat = nullptr)
 {
     LaunchCtx L;
     L.blocks = s->d_blocks;
@@ -763,6 +832,16 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     L.mol.F = dAcc;
     L.mol.nao = s->nao;
     for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
+    L.qstat = qstat;
+    if (mode != vlx::MODE_ERI && dscr_active(s)) {
+        const int rc = prepare_dscr(s, dD, st);
+        if (rc) return rc;
+        if (launches) (*launches)++;
+        L.dsh = s->d_dsh;
+        L.nsh = (int)s->shells.size();
+        L.tau_skip = (float)s->dscr_skip;
+        L.tau32 = (float)s->dscr_fp32;
+    }
     return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, ith, ith32, st, launches, events);
 }
 
@@ -1048,6 +1127,9 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_F) cudaFree(s->d_F);
     if (s->d_acc) cudaFree(s->d_acc);
     if (s->d_counters) cudaFree(s->d_counters);
+    if (s->d_dsh) cudaFree(s->d_dsh);
+    if (s->d_shinfo) cudaFree(s->d_shinfo);
+    if (s->d_qstat) cudaFree(s->d_qstat);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1234,6 +1316,10 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
                         " on this screener; run one allocating build (vlx_b200_fock_build*) with it first");
     if (ts && ts->classes.size() > (size_t)kNoallocMaxClasses)
         return fail(VLX_B200_ERR_UNSUPPORTED, "fock_build_noalloc: too many quartet classes");
+    if (dscr_active(s))
+        return fail(VLX_B200_ERR_UNSUPPORTED,
+                    "fock_build_noalloc: per-quartet density screening needs device scratch for the shell-block "
+                    "maxima; switch it off (vlx_b200_set_density_screening(s, 0, 0)) for this build");
     VLX_CUDA(cudaSetDevice(s->device));
     NoallocScratch sc;
     int rc = noalloc_scratch(s->device, &sc);
@@ -1371,9 +1457,21 @@ int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const
     return rc;
 }
 
+int vlx_b200_set_density_screening(vlx_b200_screener* s, double fp32_cutoff, double skip_cutoff)
+{
+    if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
+    if (!std::isfinite(fp32_cutoff) || !std::isfinite(skip_cutoff))
+        return fail(VLX_B200_ERR_ARGUMENT, "set_density_screening: cutoffs must be finite");
+    s->dscr_fp32 = std::max(0.0, fp32_cutoff);
+    s->dscr_skip = std::max(0.0, skip_cutoff);
+    s->ith32 = -1;
+    return VLX_B200_OK;
+}
+
 int vlx_b200_set_fp32_threshold(vlx_b200_screener* s, double cutoff, double max_abs_density)
 {
     if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
+    s->dscr_fp32 = s->dscr_skip = 0.0;
     if (cutoff <= 0.0 || max_abs_density <= 0.0) {
         s->ith32 = -1;
         return VLX_B200_OK;
@@ -1432,9 +1530,18 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         VLX_CUDA(cudaEventCreate(&e.second));
     }
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
+    // quartets and primitive quartets per class and precision, counted on the
+    // device (they depend on the density when the per-quartet screening is on)
+    if (s->nqstat < (int)(4 * nc)) {
+        if (s->d_qstat) cudaFree(s->d_qstat);
+        s->d_qstat = nullptr;
+        s->nqstat = std::max<int>(4 * (int)nc, 256);
+        VLX_CUDA(cudaMalloc(&s->d_qstat, s->nqstat * sizeof(unsigned long long)));
+    }
+    VLX_CUDA(cudaMemsetAsync(s->d_qstat, 0, 4 * nc * sizeof(unsigned long long), st));
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
     rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev);
+                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, s->d_qstat);
     if (!rc && symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
         symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
@@ -1443,6 +1550,11 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    std::vector<unsigned long long> qs(4 * nc, 0);
+    if (!rc) {
+        e = cudaMemcpy(qs.data(), s->d_qstat, qs.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+    }
     int n = 0;
     for (size_t c = 0; c < nc && !rc; c++) {
         const ClassTasks& ct = ts->classes[c];
@@ -1457,8 +1569,8 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
         p.device_ms = ms;
-        long long q = 0, q32 = 0, pq = 0;
-        count_class(s, ct, ith, s->ith32, &q, &q32, &pq);
+        const unsigned long long* c4 = &qs[4 * c];  // FP64 {quartets, prim}, FP32 {quartets, prim}
+        const long long q = (long long)(c4[0] + c4[2]), q32 = (long long)c4[2], pq = (long long)(c4[1] + c4[3]);
         p.shell_quartets = q;
         p.prim_quartets = pq;
         p.flops = class_flops(s, ct, q, pq);

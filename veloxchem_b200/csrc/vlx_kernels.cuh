@@ -209,17 +209,65 @@ template <> struct BlocksHint<0, 1, 0, 0> { static constexpr int value = 8; };
 template <> struct BlocksHint<1, 1, 0, 1> { static constexpr int value = 4; };
 template <> struct BlocksHint<0, 2, 0, 1> { static constexpr int value = 4; };
 
+// One step of a work item: lane evaluates ket pair jj of kb against the bra
+// pair (act = false: an idle lane, which computes and contributes nothing)
+// and digests the spherical block.
 template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
+__device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, const bool f32, const int lane,
+                                             const PairBlockDev& bb, const PairBlockDev& kb, const int bbi,
+                                             const int kbi, const WorkItem& w, const PairView& bra, const MolDev& m,
+                                             const int p0, const int q0, const double s_bra, const int jj,
+                                             const bool act, const double* sboys)
 {
     using C = EriClass<LA, LB, LC, LD>;
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
+    const int nlp = m.nl[LA], nlq = m.nl[LB], nlr = m.nl[LC], nls = m.nl[LD];
+    const PairView ket = make_view(kb, jj);
+    if (a.qstat) {
+        const unsigned n = __popc(__ballot_sync(0xffffffffu, act));
+        const unsigned pq = __reduce_add_sync(0xffffffffu, act ? (unsigned)(bra.kuse * ket.kuse) : 0u);
+        if (lane == 0) {
+            atomicAdd(a.qstat, (unsigned long long)n);
+            atomicAdd(a.qstat + 1, (unsigned long long)pq);
+        }
+    }
+    double f[C::NSPH];
+    if (f32) {
+        float g[C::NSPH];
+        const PairViewF braf = make_view_f(bb, w.bra, bra.kuse), ketf = make_view_f(kb, jj, ket.kuse);
+        C::compute_f32(braf, ketf, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
+#pragma unroll
+        for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
+    } else {
+        C::compute(bra, ket, sboys, a.omega2, f);
+    }
+    const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
+    const int dmode = mode & 3;
+    if (dmode == MODE_ERI) {
+        if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, m.nao);
+    } else {
+        double s = act ? s_bra : 0.0;
+        if (r0 == s0) s *= 0.5;
+        if (bbi == kbi && jj == w.bra) s *= 0.5;
+        if (dmode == MODE_FOCK_SYM)
+            digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+        else
+            digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+    }
+}
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
+{
     constexpr int L = LA + LB + LC + LD;
     const int lane = threadIdx.x & 31;
     // the Boys coefficients of the one order the class needs (the lower orders
     // follow by recursion), staged once per persistent block: the per-lane
     // table lookups then gather from shared memory instead of L1/L2
     __shared__ double sboys[BOYS_NINT * BOYS_NCOEF];
+    // per warp: kets that passed the density screening, waiting for a full step
+    __shared__ int squeue[kWarpsPerBlock][64];
+    int* queue = squeue[threadIdx.x >> 5];
     const bool f32 = (mode & MODE_F32) != 0;
     if (f32) {
         float* sf = reinterpret_cast<float*>(sboys);
@@ -240,40 +288,53 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
         const PairBlockDev bb = a.blocks[bbi];
         const PairBlockDev kb = a.blocks[kbi];
         const MolDev m = a.mols ? a.mols[bb.mol] : a.mol;
-        const int nlp = m.nl[LA], nlq = m.nl[LB], nlr = m.nl[LC], nls = m.nl[LD];
         const PairView bra = make_view(bb, w.bra);
         const int p0 = __ldg(bb.ao + w.bra), q0 = __ldg(bb.ao + bb.npairs + w.bra);
         const double s_bra = (p0 == q0) ? 0.5 : 1.0;
         int k0, k1;
-        item_range(a, bb, kb, w, (mode & MODE_F32) != 0, k0, k1);
-        for (int j0 = k0; j0 < k1; j0 += 32) {
-            const int j = j0 + lane;
-            const bool act = j < k1;
-            const int jj = act ? j : (k1 - 1);
-            const PairView ket = make_view(kb, jj);
-            double f[C::NSPH];
-            if (f32) {
-                float g[C::NSPH];
-                const PairViewF braf = make_view_f(bb, w.bra, bra.kuse), ketf = make_view_f(kb, jj, ket.kuse);
-                C::compute_f32(braf, ketf, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
-#pragma unroll
-                for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];
+        // with density screening the precision is decided per quartet below,
+        // so both launches walk the item's whole ket range
+        item_range(a, bb, kb, w, f32 && !a.dsh, k0, k1);
+        int P = 0, Q = 0;
+        float qpq = 0.0f, dpq = 0.0f;
+        if (a.dsh) {
+            P = __ldg(bb.sh + w.bra);
+            Q = __ldg(bb.sh + bb.npairs + w.bra);
+            qpq = __ldg(bb.q + w.bra);
+            dpq = __ldg(a.dsh + (size_t)P * a.nsh + Q);
+        }
+        // steps of 32 kets; with density screening the kets this launch keeps
+        // are first compacted into full steps (order preserved)
+        int n = 0, j0 = k0;
+        for (;;) {
+            int jj;
+            bool act;
+            if (!a.dsh) {
+                if (j0 >= k1) break;
+                const int j = j0 + lane;
+                act = j < k1;
+                jj = act ? j : (k1 - 1);
+                j0 += 32;
             } else {
-                C::compute(bra, ket, sboys, a.omega2, f);
+                while (n < 32 && j0 < k1) {
+                    const int j = j0 + lane;
+                    const bool keep = (j < k1) && quartet_kept(a, quartet_bound(a, P, Q, qpq, dpq, kb, j), f32);
+                    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                    if (keep) queue[n + __popc(mask & ((1u << lane) - 1u))] = j;
+                    n += __popc(mask);
+                    j0 += 32;
+                    __syncwarp();
+                }
+                if (n == 0) break;
+                act = lane < n;
+                jj = queue[act ? lane : 0];
+                __syncwarp();
+                if (lane < n - 32) queue[lane] = queue[lane + 32];
+                n = max(n - 32, 0);
+                __syncwarp();
             }
-            const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
-            const int dmode = mode & 3;
-            if (dmode == MODE_ERI) {
-                if (act) scatter_eri<NA, NB, NC, ND>(f, p0, nlp, q0, nlq, r0, nlr, s0, nls, a.eri, m.nao);
-            } else {
-                double s = act ? s_bra : 0.0;
-                if (r0 == s0) s *= 0.5;
-                if (bbi == kbi && jj == w.bra) s *= 0.5;
-                if (dmode == MODE_FOCK_SYM)
-                    digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
-                else
-                    digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
-            }
+            quartet_step<LA, LB, LC, LD>(a, mode, f32, lane, bb, kb, bbi, kbi, w, bra, m, p0, q0, s_bra, jj, act,
+                                         sboys);
         }
     }
 }

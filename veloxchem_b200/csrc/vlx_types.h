@@ -34,6 +34,8 @@ struct PairBlockDev {
     const int* nuse;     // [npairs]     primitive pairs with |kfac| >= VLX_PRIM_CUTOFF
     const int* bin;      // [npairs]     Schwarz bin of the pair (pairs sorted by bin)
     const int* bin_off;  // [17]         first pair of bin b (pairs with bin <= b end at bin_off[b + 1])
+    const int* sh;       // [2][npairs]  shell index of A and of B (rows / columns of FockArgs::dsh)
+    const float* q;      // [npairs]     Schwarz factor sqrt(max (ab|ab)), rounded up
     int npairs;
     int kprim;
     int la, lb;
@@ -75,6 +77,14 @@ struct FockArgs {
     double omega2;            // 0: Coulomb; > 0: erf(omega r)/r with omega^2 (labels j_rs, k_rs, kx_rs)
     int ith;                  // quartets with bin_bra + bin_ket <= ith are evaluated (run-time filter)
     int ith32;                // those with bin_bra + bin_ket >= ith32 in FP32 (-1: none)
+    // per-quartet density screening (dsh != nullptr): the bound of (PQ|RS) is
+    // q_PQ q_RS max(|cj| max(d_PQ, d_RS), |ck| max(d_PR, d_PS, d_QR, d_QS)),
+    // d the shell-block maxima of |D|; quartets below tau_skip are skipped,
+    // those below tau32 are the FP32 launch's, the rest the FP64 launch's
+    const float* dsh;         // nsh x nsh, max over the two orientations of the block
+    int nsh;
+    float tau_skip, tau32;
+    unsigned long long* qstat;  // [2] quartets and primitive quartets evaluated by the launch (nullptr: off)
 };
 
 }  // namespace vlx

@@ -23,9 +23,9 @@ scfrestdriver.py) for the parts a restricted HF energy needs:
   D = C_occ C_occ^T (scfrestdriver.py:214-269);
 * convergence when the electronic gradient is below ``conv_thresh``
   (default 1e-6, scfdriver.py:151);
-* incremental Fock builds with density-difference screening (the reference
-  SCF builds from the full density each iteration); convergence is always
-  confirmed on a full FP64 build.
+* incremental Fock builds with per-quartet density-difference screening (the
+  reference SCF builds from the full density each iteration); convergence is
+  always confirmed on a full FP64 build with the reference's screening.
 
 Linear algebra runs in FP64 with torch on the same GPU; the Fock build is the
 native library's.
@@ -121,9 +121,12 @@ class ScfRestrictedDriver:
         self.ovl_thresh = 1.0e-6
         self.guess = 'sad'
         self.guess_weights = None  # learned guess: network file (default: the shipped def2-SVP water model)
-        # mixed precision: quartets with Schwarz bound x max|D| < fp32_cutoff in
-        # FP32 while the electronic gradient is above fp32_until_grad; the
-        # final iterations are FP64, so the converged energy is the FP64 one
+        # mixed precision: quartets whose density-weighted bound (the Schwarz
+        # factors times the local shell-block maxima of |D|) is below
+        # fp32_cutoff in FP32 -- in full builds while the electronic gradient
+        # is above fp32_until_grad, in incremental builds throughout (their
+        # FP32 error scales with |dD|); convergence is confirmed on a full FP64
+        # build, so the converged energy is the FP64 one
         self.fp32_cutoff = 0.0
         self.fp32_until_grad = 1.0e-4
         # early iterations (until the electronic gradient first drops to
@@ -136,15 +139,18 @@ class ScfRestrictedDriver:
         self.early_ithreshold = None
         self.early_until_grad = 1.0e-2
         self.early_fp32_cutoff = 1.0e-4
-        # incremental Fock builds: F_n = F_(n-1) + G(D_n - D_(n-1)) with the
-        # screening threshold tightened by max|D_n - D_(n-1)| (a quartet is
-        # dropped when its Schwarz bound times max|dD| is below a hundredth of
-        # the dynamic threshold); a full build every rebuild_every iterations,
-        # whenever the dynamic threshold changes, and to confirm convergence;
-        # after a convergence check that the full build does not confirm, the
-        # remaining iterations use full builds
+        # incremental Fock builds: F_n = F_(n-1) + G(D_n - D_(n-1)) with
+        # per-quartet density screening on dD = D_n - D_(n-1) (a quartet is
+        # skipped when sqrt((PQ|PQ)(RS|RS)) times the weighted local maxima of
+        # |dD| is below inc_skip_factor times the dynamic threshold, and, in
+        # mixed precision, evaluated in FP32 below fp32_cutoff); a full build
+        # every rebuild_every iterations, whenever the dynamic threshold
+        # changes, and to confirm convergence; after a convergence check that
+        # the full build does not confirm, the remaining iterations use full
+        # builds
         self.incremental = True
         self.rebuild_every = 8
+        self.inc_skip_factor = 1.0e-2
         self.history = []
         self.timings = {}
 
@@ -233,14 +239,13 @@ class ScfRestrictedDriver:
             dl = torch.from_numpy(D_l).to(dev)
             dl = 0.5 * (dl + dl.T).contiguous()
             fl = torch.empty_like(dl)
-            screener.set_fp32_threshold(self._fp32_cutoff(self.early_ithreshold is not None),
-                                        float(torch.max(torch.abs(dl))))
+            screener.set_density_screening(self._fp32_cutoff(self.early_ithreshold is not None), 0.0)
             build(dl, fl, ith0)
             ds = 0.5 * (D + D.T).contiguous()
             fs = torch.empty_like(ds)
-            screener.set_fp32_threshold(1.0e-4, float(torch.max(torch.abs(ds))))
+            screener.set_density_screening(1.0e-4, 0.0)
             build(ds, fs, min(ith0, 6))
-            screener.set_fp32_threshold(0.0, 0.0)
+            screener.set_density_screening(0.0, 0.0)
             e_l = float(torch.sum(dl * fl) + 2.0 * torch.sum(dl * H))
             e_s = float(torch.sum(ds * fs) + 2.0 * torch.sum(ds * H))
             torch.cuda.synchronize(dev)
@@ -286,14 +291,16 @@ class ScfRestrictedDriver:
                 ith_used = ith
             elif inc:
                 dD = (D - D_prev).contiguous()
-                m = float(torch.max(torch.abs(dD)))
-                ith_used = min(ith, max(0, ith + 2 + math.floor(math.log10(m)))) if m > 0.0 else ith
-                screener.set_fp32_threshold(cutoff, m)
-                build(dD, G, ith_used)
+                # the FP32 error of an incremental build scales with |dD|, so
+                # its small quartets stay FP32 until convergence
+                screener.set_density_screening(self._fp32_cutoff(early) if self.fp32_cutoff > 0.0 else 0.0,
+                                               self.inc_skip_factor * 10.0 ** (-ith))
+                build(dD, G, ith)
+                ith_used = ith
                 F2e.copy_(F2e_prev)
                 F2e.add_(G)
             else:
-                screener.set_fp32_threshold(cutoff, float(torch.max(torch.abs(D))))
+                screener.set_density_screening(cutoff, 0.0)
                 build(D, F2e, ith)
                 ith_used = ith
             torch.cuda.synchronize(dev)
@@ -309,7 +316,7 @@ class ScfRestrictedDriver:
             if e_grad < self.conv_thresh and inc and not early:
                 # confirm on a full FP64 build of the same density
                 t0 = time.perf_counter()
-                screener.set_fp32_threshold(0.0, 0.0)
+                screener.set_density_screening(0.0, 0.0)
                 build(D, F2e, ith)
                 torch.cuda.synchronize(dev)
                 fock_ms += 1e3 * (time.perf_counter() - t0)
@@ -336,7 +343,7 @@ class ScfRestrictedDriver:
             D = C @ C.T
             torch.cuda.synchronize(dev)
             eigh_s += time.perf_counter() - t0
-        screener.set_fp32_threshold(0.0, 0.0)
+        screener.set_density_screening(0.0, 0.0)
         self.timings['fock_ms_total'] = fock_ms
         self.timings['diag_s'] = eigh_s
         self.timings['total_s'] = time.perf_counter() - t_start

@@ -113,6 +113,14 @@ class T4CScreener:
         nat.check(nat.lib().vlx_b200_set_fp32_threshold(self.handle, float(cutoff), float(max_abs_density)),
                   'set_fp32_threshold')
 
+    def set_density_screening(self, fp32_cutoff=0.0, skip_cutoff=0.0):
+        """Per-quartet screening of the following builds on the bound
+        sqrt((PQ|PQ)(RS|RS)) x (local shell-block maxima of |D|): quartets
+        below skip_cutoff are skipped, those below fp32_cutoff evaluated in
+        FP32 (0 switches a part off; both 0: the reference's screening)."""
+        nat.check(nat.lib().vlx_b200_set_density_screening(self.handle, float(fp32_cutoff), float(skip_cutoff)),
+                  'set_density_screening')
+
     def set_work_threshold(self, ithreshold_base):
         """Build work lists for max(ithreshold, ithreshold_base) and filter at
         run time, so builds at several thresholds share one list."""
