@@ -107,14 +107,20 @@ int vlx_b200_fock_build(vlx_b200_screener* screener, const double* density, int 
                         vlx_b200_stats* stats);
 
 /* The share of the build of rank `rank` out of `nodes` (work items dealt
- * round-robin); the sum over ranks equals vlx_b200_fock_build.
+ * round-robin by default, see vlx_b200_set_partition); the sum over ranks
+ * equals vlx_b200_fock_build.
  * Replaces CFockDriver::compute(screener, rank, nodes, density, ...)
  * (src/t4c_func/FockDriver.cpp:234-290). */
 int vlx_b200_fock_build_local(vlx_b200_screener* screener, int rank, int nodes, const double* density,
                               int symmetric, const char* label, double exchange_factor, double omega,
                               int ithreshold, double* fock_out, vlx_b200_stats* stats);
 
-/* Several densities, one label each, in one pass over the quartets.
+/* Several densities, one label each, in one pass over the quartets: every
+ * evaluated quartet is digested into each density's Fock matrix (up to 8
+ * densities per pass; more take one pass per 8).  As in the reference the
+ * operator is erf(omega r) / r only when every label is range-separated,
+ * otherwise all densities take the Coulomb integrals.  The per-quartet
+ * density screening (vlx_b200_set_density_screening) does not apply here.
  * densities / focks_out: ndens host matrices of nao x nao.
  * Replaces CFockDriver::compute(screener, densities, labels, ...)
  * (src/t4c_func/FockDriver.cpp:176-230) and its rank/nodes overload (:294-352)

@@ -50,7 +50,6 @@ def test_h2o32_svp_against_reference():
         assert np.max(np.abs(f - r)) < TOL, label
 
 
-@pytest.mark.skipif(not (GOLDEN / 'h2o64_tzvp_jk.npz').exists(), reason='fixture not generated yet')
 def test_h2o64_tzvp_against_reference_fixture():
     from veloxchem_b200 import FockDriver, MolecularBasis, T4CScreener, make_matrix, mat_t
     from veloxchem_b200.geometry import random_density, water_cluster

@@ -201,3 +201,27 @@ def test_scf_threshold_schedule():
     assert drv._fp32_cutoff(True) == 0.0  # mixed precision off: no FP32 at all
     drv.fp32_cutoff = 1e-6
     assert drv._fp32_cutoff(True) == 1e-4 and drv._fp32_cutoff(False) == 1e-6
+
+
+def test_c2diis_weights_find_the_zero_residual_combination():
+    """C2-DIIS picks the unit-sum eigenvector of the error overlap matrix with
+    the smallest residual: for error vectors e and -e/3 that is the exact
+    cancellation w = (1/4, 3/4), applied to the Fock matrices."""
+    import torch
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    rng = np.random.default_rng(0)
+    e = torch.from_numpy(rng.standard_normal((6, 6)))
+    f1, f2 = torch.ones((6, 6), dtype=torch.float64), 2.0 * torch.ones((6, 6), dtype=torch.float64)
+    out = ScfRestrictedDriver._c2diis([f1, f2], [e, -e / 3.0])
+    assert torch.allclose(out, 0.25 * f1 + 0.75 * f2, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_scf_energy_known_answer_c2diis():
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol, bas = _dimer()
+    drv = ScfRestrictedDriver()
+    drv.acc_type = 'c2diis'
+    res = drv.compute(mol, bas)
+    assert res['converged']
+    assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8

@@ -191,7 +191,28 @@ class ClassGen:
                 out.append('%s * hizh * %s' % (_num(t[1]), n[t[2]]))
         return ' + '.join(out)
 
-    def emit(self, real='double'):
+    def closure(self, keys):
+        """VRR nodes the given nodes depend on (themselves included), in the
+        emission order."""
+        seen, stack = set(), list(keys)
+        while stack:
+            k = stack.pop()
+            if k in seen:
+                continue
+            seen.add(k)
+            for term in self.vrr.nodes[k]:
+                for x in term[2:]:
+                    if isinstance(x, tuple):
+                        stack.append(x)
+        return [k for k in self.vrr.order if k in seen]
+
+    def emit(self, real='double', parts=1):
+        """parts > 1: the accumulator rows (bra Cartesian targets e) are
+        evaluated in `parts` groups, each with its own primitive loop over only
+        the recursion nodes its rows need, and ket-transformed into the
+        half-transformed values h_e_k_l before the next group starts, so that
+        only one group's accumulators are live at a time (for classes whose
+        contracted buffer does not fit the registers)."""
         la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
         L = self.L
         na, nb, nc, nd = 2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1
@@ -208,10 +229,39 @@ class ClassGen:
         w('    __device__ __forceinline__ static void compute(const BraT& bra, const KetT& ket, const double* __restrict__ btab,')
         w('                                                   const double om2, double* __restrict__ out)')
         w('    {')
-        for ie in range(len(e_t)):
+        groups = [list(range(len(e_t)))[r::parts] for r in range(parts)]
+        if parts > 1:
+            for ie in range(len(e_t)):
+                for k in range(nc):
+                    for l in range(nd):
+                        w('        double h_%d_%d_%d;' % (ie, k, l))
+        w('        const int kb = bra.nprim(), kk = ket.nprim();')
+        for group in groups:
+            self._emit_group(w, group, parts > 1)
+        if parts > 1:
+            w('        const double BAx = bra.abx(), BAy = bra.aby(), BAz = bra.abz();')
+            w('        (void)BAx; (void)BAy; (void)BAz;')
+        self._emit_bra(w)
+        if parts == 1:
+            w('        }')
+        w('    }')
+        body = lines[method_start:]
+        lines.extend(to_f32(body))
+        w('};')
+        return '\n'.join(lines)
+
+    def _emit_group(self, w, group, store):
+        """Primitive loop and ket transform of the accumulator rows `group`
+        (indices into e_targets); store: assign to the function-scope h_e_k_l
+        (grouped emission) instead of declaring them."""
+        la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
+        L = self.L
+        nc, nd = 2 * lc + 1, 2 * ld + 1
+        e_t, f_t = self.e_targets, self.f_targets
+        w('        {')
+        for ie in group:
             for jf in range(len(f_t)):
                 w('        double c_%d_%d = 0.0;' % (ie, jf))
-        w('        const int kb = bra.nprim(), kk = ket.nprim();')
         # ket primitives outer: the ket data is per lane (loaded once per ket
         # primitive), the bra data is warp-uniform (broadcast loads)
         w('        for (int pk = 0; pk < kk; pk++) {')
@@ -244,17 +294,20 @@ class ClassGen:
         w('                (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;')
         w('                (void)QDx; (void)QDy; (void)QDz; (void)PBx; (void)PBy; (void)PBz;')
         w('                (void)hiz; (void)hie; (void)hizh; (void)rz; (void)rh;')
-        for key in self.vrr.order:
+        needed = self.closure([(e_t[ie], f, 0) for ie in group for f in f_t])
+        for key in needed:
             w('                const double %s = %s;' % (self.names[key], self._vrr_expr(key)))
-        for ie, e in enumerate(e_t):
+        for ie in group:
             for jf, f in enumerate(f_t):
-                w('                c_%d_%d += %s;' % (ie, jf, self.names[(e, f, 0)]))
+                w('                c_%d_%d += %s;' % (ie, jf, self.names[(e_t[ie], f, 0)]))
         w('            }')
         w('        }')
         # ---- ket HRR (per e target) then ket spherical
         w('        const double DCx = ket.abx(), DCy = ket.aby(), DCz = ket.abz();')
-        w('        const double BAx = bra.abx(), BAy = bra.aby(), BAz = bra.abz();')
-        w('        (void)DCx; (void)DCy; (void)DCz; (void)BAx; (void)BAy; (void)BAz;')
+        w('        (void)DCx; (void)DCy; (void)DCz;')
+        if not store:
+            w('        const double BAx = bra.abx(), BAy = bra.aby(), BAz = bra.abz();')
+            w('        (void)BAx; (void)BAy; (void)BAz;')
         f_index = {f: j for j, f in enumerate(f_t)}
         ket_nodes, ket_order = {}, []
 
@@ -277,7 +330,7 @@ class ClassGen:
                 need_ket(c, d)
         sph_c, sph_d = sph_coefficients(lc), sph_coefficients(ld)
         # half-transformed buffer h[ie][k][l]
-        for ie in range(len(e_t)):
+        for ie in group:
             names = {}
             for n_, key in enumerate(ket_order):
                 node = ket_nodes[key]
@@ -297,7 +350,15 @@ class ClassGen:
                             if sph_d[l][jd] == 0.0:
                                 continue
                             terms.append('%s * %s' % (_num(sph_c[k][ic] * sph_d[l][jd]), names[(c, d)]))
-                    w('        const double h_%d_%d_%d = %s;' % (ie, k, l, ' + '.join(terms)))
+                    w('        %sh_%d_%d_%d = %s;' % ('' if store else 'const double ', ie, k, l, ' + '.join(terms)))
+        if not store:
+            return  # single group: the bra part follows in the same scope
+        w('        }')
+
+    def _emit_bra(self, w):
+        la, lb, lc, ld = self.la, self.lb, self.lc, self.ld
+        na, nb, nc, nd = 2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1
+        e_t = self.e_targets
         # ---- bra HRR per (k, l), then bra spherical
         e_index = {e: j for j, e in enumerate(e_t)}
         bra_nodes, bra_order = {}, []
@@ -342,11 +403,6 @@ class ClassGen:
                                     continue
                                 terms.append('%s * %s' % (_num(sph_a[i][ia] * sph_b[j][jb]), names[(a, b)]))
                         w('        out[%d] = %s;' % (((i * nb + j) * nc + k) * nd + l, ' + '.join(terms)))
-        w('    }')
-        body = lines[method_start:]
-        lines.extend(to_f32(body))
-        w('};')
-        return '\n'.join(lines)
 
 
 
@@ -514,6 +570,7 @@ def to_f32(method_lines):
         t = t.replace('const double* __restrict__ btab', 'const float* __restrict__ btab')
         t = t.replace('double* __restrict__ out', 'float* __restrict__ out')
         t = t.replace('const double ', 'const float ').replace('double c_', 'float c_').replace('double F[', 'float F[')
+        t = t.replace('double h_', 'float h_')
         t = t.replace('boys_function_tab<', 'boys_function_tab_f<').replace('rsqrt(', 'rsqrtf(')
         t = re.sub(r'(?<![r\w])sqrt\(', 'sqrtf(', t).replace('double pref', 'float pref')
         if not t.lstrip().startswith('//'):
@@ -564,18 +621,23 @@ def emit_class_file(cls, outdir):
     w('// Generated by gen_eri.py -- do not edit.')
     w('#include "vlx_kernels.cuh"')
     w('namespace vlx {')
-    w(g.emit())
+    w(g.emit(parts=class_parts(cls)))
     w('')
     w('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st)' % nm)
     w('{')
     w('    const dim3 blk(32 * kWarpsPerBlock);')
-    w('    quartet_kernel_of<%d, %d, %d, %d>()<<<grid, blk, 0, st>>>(a, mode);' % cls)
+    w('    if (needs_ext(a))')
+    w('        quartet_kernel_of<%d, %d, %d, %d, true>()<<<grid, blk, 0, st>>>(a, mode);' % cls)
+    w('    else')
+    w('        quartet_kernel_of<%d, %d, %d, %d, false>()<<<grid, blk, 0, st>>>(a, mode);' % cls)
     w('}')
-    w('int occupancy_quartet_%s(int mode)' % nm)
+    w('int occupancy_quartet_%s(int ext)' % nm)
     w('{')
     w('    int n = 0;')
-    w('    (void)mode;')
-    w('    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel_of<%d, %d, %d, %d>(), 32 * kWarpsPerBlock, 0);' % cls)
+    w('    if (ext)')
+    w('        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel_of<%d, %d, %d, %d, true>(), 32 * kWarpsPerBlock, 0);' % cls)
+    w('    else')
+    w('        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, quartet_kernel_of<%d, %d, %d, %d, false>(), 32 * kWarpsPerBlock, 0);' % cls)
     w('    return n;')
     w('}')
     if (la, lb) == (lc, ld):
@@ -595,9 +657,24 @@ VRR_COMPILED_MAX = 2400
 ACC_COMPILED_MAX = 180
 
 
+# Classes beyond the register budget that are compiled all the same (the
+# compiler keeps what does not fit the registers in thread-local memory),
+# with the number of accumulator groups of ClassGen.emit: measured faster
+# than the warp-cooperative kernel on the (H2O)64 / def2-TZVP build.
+GROUPED = {(1, 3, 1, 1): 1, (1, 3, 0, 3): 1, (3, 3, 0, 1): 1, (2, 2, 1, 1): 1, (2, 2, 0, 2): 1, (2, 3, 0, 2): 1,
+           (1, 2, 1, 2): 1, (2, 2, 0, 3): 1, (1, 3, 1, 2): 3, (2, 3, 1, 1): 2}
+
+
+def class_parts(cls):
+    return GROUPED.get(tuple(cls), 1)
+
+
 def is_compiled(cls):
-    """Straight-line register kernel when the contracted buffer and the
-    recursion graph are small enough; otherwise the warp-cooperative kernel."""
+    """Straight-line per-lane kernel when the contracted buffer and the
+    recursion graph are small enough, or the class is listed in GROUPED;
+    otherwise the warp-cooperative kernel."""
+    if tuple(cls) in GROUPED:
+        return True
     g = ClassGen(*cls)
     return len(g.vrr.order) <= VRR_COMPILED_MAX and len(g.e_targets) * len(g.f_targets) <= ACC_COMPILED_MAX
 

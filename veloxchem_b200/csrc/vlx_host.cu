@@ -376,6 +376,8 @@ struct vlx_b200_screener {
     int2* d_shinfo = nullptr;    // per shell: AO index of component 0, angular momentum
     unsigned long long* d_qstat = nullptr;  // profiled builds: [class][FP64, FP32][quartets, primitive quartets]
     int nqstat = 0;
+    double* d_multi = nullptr;  // multi-density builds: densities / outputs, then accumulators
+    int nmulti = 0;
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -735,6 +737,7 @@ struct LaunchCtx {
     int nsh = 0;
     float tau_skip = 0.0f, tau32 = 0.0f;
     unsigned long long* qstat = nullptr;  // [class][FP64, FP32][2] quartet counters (profiled builds)
+    vlx::DensSet dens{};                  // multi-density build (dens.n > 0)
 };
 
 // Enqueues all class kernels of a task set on `st`; the accumulators must be
@@ -763,6 +766,7 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.ith32 = L.dsh ? -1 : ith32;
     a.dsh = L.dsh;
     a.nsh = L.nsh;
+    a.dens = L.dens;
     a.tau_skip = L.tau_skip;
     a.tau32 = L.tau32;
     const int nprec = (L.dsh ? L.tau32 > 0.0f : ith32 >= 0) ? 2 : 1;
@@ -781,7 +785,7 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
             const int fmode = f ? (mode | vlx::MODE_F32) : mode;
             if (ct.compiled >= 0) {
                 const auto& e = vlx::kQuartetClasses[ct.compiled];
-                const int occ = std::max(1, e.occupancy(mode));
+                const int occ = std::max(1, e.occupancy(vlx::needs_ext(af) ? 1 : 0));
                 const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
                 e.launch(fmode, af, std::max(1, std::min(want, occ * nsm)), st);
             } else {
@@ -1130,6 +1134,7 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_dsh) cudaFree(s->d_dsh);
     if (s->d_shinfo) cudaFree(s->d_shinfo);
     if (s->d_qstat) cudaFree(s->d_qstat);
+    if (s->d_multi) cudaFree(s->d_multi);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1206,19 +1211,93 @@ int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int nde
                               double* const* focks_out, vlx_b200_stats* stats)
 {
     if (!s || ndens < 1 || !densities || !labels || !focks_out) return fail(VLX_B200_ERR_ARGUMENT, "null argument");
-    vlx_b200_stats acc{};
+    for (int i = 0; i < ndens; i++)
+        if (!densities[i] || !focks_out[i]) return fail(VLX_B200_ERR_ARGUMENT, "null density or Fock matrix");
+    if (nodes < 1 || rank < 0 || rank >= nodes) return fail(VLX_B200_ERR_ARGUMENT, "invalid rank / nodes");
+    if (!std::isfinite(omega) || omega < 0.0) return fail(VLX_B200_ERR_ARGUMENT, "omega must be finite and >= 0");
+    const auto t0 = std::chrono::steady_clock::now();
+    VLX_CUDA(cudaSetDevice(s->device));
+    // the operator is erf(omega r) / r only when every label is range-separated
+    // (CT4CMatricesDistributor::need_omega, T4CMatricesDistributor.cpp:55-66);
+    // otherwise all densities take the Coulomb integrals
+    bool all_rs = true;
+    for (int i = 0; i < ndens; i++) all_rs = all_rs && label_is_range_separated(labels[i]);
+    const double omega2 = all_rs ? omega * omega : 0.0;
+    std::vector<double> cj(ndens, 0.0), ck(ndens, 0.0);
+    bool any = false;
     for (int i = 0; i < ndens; i++) {
-        vlx_b200_stats one{};
-        const int rc = host_build(s, rank, nodes, densities[i], symmetric, labels[i], xfac, omega, ith, focks_out[i],
-                                  &one);
-        if (rc) return rc;
-        acc.device_ms += one.device_ms;
-        acc.total_ms += one.total_ms;
-        acc.shell_quartets += one.shell_quartets;
-        acc.prim_quartets += one.prim_quartets;
-        acc.kernel_launches += one.kernel_launches;
+        const bool known = label_weights(labels[i], symmetric, xfac, &cj[i], &ck[i]) && !(all_rs && omega == 0.0);
+        if (!known) cj[i] = ck[i] = 0.0;
+        any = any || known;
     }
-    if (stats) *stats = acc;
+    const size_t nn = (size_t)s->nao * s->nao, bytes = nn * sizeof(double);
+    const int chunk = std::min(ndens, vlx::kMaxDens);
+    if (s->nmulti < chunk) {
+        if (s->d_multi) cudaFree(s->d_multi);
+        s->d_multi = nullptr;
+        VLX_CUDA(cudaMalloc(&s->d_multi, 2 * (size_t)chunk * std::max<size_t>(bytes, 8)));
+        s->nmulti = chunk;
+    }
+    TaskSet* ts = nullptr;
+    if (any) {
+        const int rc = build_tasks(s, ith, rank, nodes, &ts);
+        if (rc) return rc;
+    }
+    vlx_b200_stats acc{};
+    VLX_CUDA(cudaEventRecord(s->ev0, s->stream));
+    for (int c0 = 0; c0 < ndens; c0 += vlx::kMaxDens) {
+        const int nd = std::min(vlx::kMaxDens, ndens - c0);
+        double* dD = s->d_multi;                      // nd densities, then the outputs
+        double* dA = s->d_multi + (size_t)chunk * nn;  // nd accumulators
+        LaunchCtx L;
+        L.blocks = s->d_blocks;
+        L.glob = s->glob;
+        L.counters = s->d_counters;
+        L.mol.D = dD;
+        L.mol.F = dA;
+        L.mol.nao = s->nao;
+        for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
+        L.dens.n = nd;
+        bool chunk_any = false;
+        for (int d = 0; d < nd; d++) {
+            VLX_CUDA(cudaMemcpyAsync(dD + d * nn, densities[c0 + d], bytes, cudaMemcpyHostToDevice, s->stream));
+            L.dens.D[d] = dD + d * nn;
+            L.dens.F[d] = dA + d * nn;
+            L.dens.cj[d] = cj[c0 + d];
+            L.dens.ck[d] = ck[c0 + d];
+            chunk_any = chunk_any || cj[c0 + d] != 0.0 || ck[c0 + d] != 0.0;
+        }
+        VLX_CUDA(cudaMemsetAsync(dA, 0, nd * bytes, s->stream));
+        if (chunk_any && ts) {
+            // one pass over the quartets digests every density of the chunk
+            const int rc = enqueue_ctx(L, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, nullptr, 1.0, 1.0,
+                                       omega2, ith, -1, s->stream, &acc.kernel_launches);
+            if (rc) return rc;
+            acc.shell_quartets += ts->quartets;
+            acc.prim_quartets += ts->prim_quartets;
+        }
+        for (int d = 0; d < nd; d++) {
+            // the density slot takes the output once the class kernels are done (stream order)
+            if (symmetric) {
+                const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
+                symmetrize_kernel<<<grid, blk, 0, s->stream>>>(dA + d * nn, dD + d * nn, s->nao);
+                VLX_CUDA(cudaGetLastError());
+                acc.kernel_launches++;
+                VLX_CUDA(cudaMemcpyAsync(focks_out[c0 + d], dD + d * nn, bytes, cudaMemcpyDeviceToHost, s->stream));
+            } else {
+                VLX_CUDA(cudaMemcpyAsync(focks_out[c0 + d], dA + d * nn, bytes, cudaMemcpyDeviceToHost, s->stream));
+            }
+        }
+    }
+    VLX_CUDA(cudaEventRecord(s->ev1, s->stream));
+    VLX_CUDA(cudaStreamSynchronize(s->stream));
+    if (stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        acc.device_ms = ms;
+        acc.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        *stats = acc;
+    }
     return VLX_B200_OK;
 }
 
@@ -1530,18 +1609,22 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         VLX_CUDA(cudaEventCreate(&e.second));
     }
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
-    // quartets and primitive quartets per class and precision, counted on the
-    // device (they depend on the density when the per-quartet screening is on)
-    if (s->nqstat < (int)(4 * nc)) {
+    // with the per-quartet density screening the evaluated quartets depend on
+    // the density: they are counted on the device (per class and precision);
+    // otherwise on the host from the work items, and the kernels profiled are
+    // the plain ones
+    const bool dev_count = dscr_active(s);
+    if (dev_count && s->nqstat < (int)(4 * nc)) {
         if (s->d_qstat) cudaFree(s->d_qstat);
+    if (s->d_multi) cudaFree(s->d_multi);
         s->d_qstat = nullptr;
         s->nqstat = std::max<int>(4 * (int)nc, 256);
         VLX_CUDA(cudaMalloc(&s->d_qstat, s->nqstat * sizeof(unsigned long long)));
     }
-    VLX_CUDA(cudaMemsetAsync(s->d_qstat, 0, 4 * nc * sizeof(unsigned long long), st));
+    if (dev_count) VLX_CUDA(cudaMemsetAsync(s->d_qstat, 0, 4 * nc * sizeof(unsigned long long), st));
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
     rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, s->d_qstat);
+                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, dev_count ? s->d_qstat : nullptr);
     if (!rc && symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
         symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
@@ -1551,7 +1634,7 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     cudaError_t e = cudaStreamSynchronize(st);
     if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     std::vector<unsigned long long> qs(4 * nc, 0);
-    if (!rc) {
+    if (!rc && dev_count) {
         e = cudaMemcpy(qs.data(), s->d_qstat, qs.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     }
@@ -1569,8 +1652,15 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
         p.device_ms = ms;
-        const unsigned long long* c4 = &qs[4 * c];  // FP64 {quartets, prim}, FP32 {quartets, prim}
-        const long long q = (long long)(c4[0] + c4[2]), q32 = (long long)c4[2], pq = (long long)(c4[1] + c4[3]);
+        long long q = 0, q32 = 0, pq = 0;
+        if (dev_count) {
+            const unsigned long long* c4 = &qs[4 * c];  // FP64 {quartets, prim}, FP32 {quartets, prim}
+            q = (long long)(c4[0] + c4[2]);
+            q32 = (long long)c4[2];
+            pq = (long long)(c4[1] + c4[3]);
+        } else {
+            count_class(s, ct, ith, s->ith32, &q, &q32, &pq);
+        }
         p.shell_quartets = q;
         p.prim_quartets = pq;
         p.flops = class_flops(s, ct, q, pq);

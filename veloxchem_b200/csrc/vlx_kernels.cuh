@@ -212,7 +212,11 @@ template <> struct BlocksHint<0, 2, 0, 1> { static constexpr int value = 4; };
 // One step of a work item: lane evaluates ket pair jj of kb against the bra
 // pair (act = false: an idle lane, which computes and contributes nothing)
 // and digests the spherical block.
-template <int LA, int LB, int LC, int LD>
+// EXT = false: the plain build (one density, the reference's screening);
+// EXT = true adds the per-quartet density screening, multi-density digestion
+// and the device quartet counters, in a separate instantiation so that the
+// plain kernels keep their code and registers.
+template <int LA, int LB, int LC, int LD, bool EXT>
 __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, const bool f32, const int lane,
                                              const PairBlockDev& bb, const PairBlockDev& kb, const int bbi,
                                              const int kbi, const WorkItem& w, const PairView& bra, const MolDev& m,
@@ -223,7 +227,7 @@ __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, 
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
     const int nlp = m.nl[LA], nlq = m.nl[LB], nlr = m.nl[LC], nls = m.nl[LD];
     const PairView ket = make_view(kb, jj);
-    if (a.qstat) {
+    if (EXT && a.qstat) {
         const unsigned n = __popc(__ballot_sync(0xffffffffu, act));
         const unsigned pq = __reduce_add_sync(0xffffffffu, act ? (unsigned)(bra.kuse * ket.kuse) : 0u);
         if (lane == 0) {
@@ -249,14 +253,34 @@ __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, 
         double s = act ? s_bra : 0.0;
         if (r0 == s0) s *= 0.5;
         if (bbi == kbi && jj == w.bra) s *= 0.5;
-        if (dmode == MODE_FOCK_SYM)
-            digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
-        else
-            digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+        if constexpr (!EXT) {
+            if (dmode == MODE_FOCK_SYM)
+                digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+            else
+                digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+            return;
+        }
+        // one density, or each density of a multi-density build in turn
+        const int nd = a.dens.n > 0 ? a.dens.n : 1;
+#pragma unroll 1
+        for (int d = 0; d < nd; d++) {
+            MolDev md = m;
+            double cj = a.cj, ck = a.ck;
+            if (a.dens.n > 0) {
+                md.D = a.dens.D[d];
+                md.F = a.dens.F[d];
+                cj = a.dens.cj[d];
+                ck = a.dens.ck[d];
+            }
+            if (dmode == MODE_FOCK_SYM)
+                digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, md, cj, ck);
+            else
+                digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, md, cj, ck);
+        }
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, bool EXT>
 __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
 {
     constexpr int L = LA + LB + LC + LD;
@@ -265,9 +289,6 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
     // follow by recursion), staged once per persistent block: the per-lane
     // table lookups then gather from shared memory instead of L1/L2
     __shared__ double sboys[BOYS_NINT * BOYS_NCOEF];
-    // per warp: kets that passed the density screening, waiting for a full step
-    __shared__ int squeue[kWarpsPerBlock][64];
-    int* queue = squeue[threadIdx.x >> 5];
     const bool f32 = (mode & MODE_F32) != 0;
     if (f32) {
         float* sf = reinterpret_cast<float*>(sboys);
@@ -292,6 +313,19 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
         const int p0 = __ldg(bb.ao + w.bra), q0 = __ldg(bb.ao + bb.npairs + w.bra);
         const double s_bra = (p0 == q0) ? 0.5 : 1.0;
         int k0, k1;
+        if constexpr (!EXT) {
+            item_range(a, bb, kb, w, f32, k0, k1);
+            for (int j0 = k0; j0 < k1; j0 += 32) {
+                const int j = j0 + lane;
+                const bool act = j < k1;
+                quartet_step<LA, LB, LC, LD, false>(a, mode, f32, lane, bb, kb, bbi, kbi, w, bra, m, p0, q0, s_bra,
+                                                    act ? j : (k1 - 1), act, sboys);
+            }
+            continue;
+        }
+        // per warp: kets that passed the density screening, waiting for a full step
+        __shared__ int squeue[kWarpsPerBlock][64];
+        int* queue = squeue[threadIdx.x >> 5];
         // with density screening the precision is decided per quartet below,
         // so both launches walk the item's whole ket range
         item_range(a, bb, kb, w, f32 && !a.dsh, k0, k1);
@@ -333,33 +367,40 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
                 n = max(n - 32, 0);
                 __syncwarp();
             }
-            quartet_step<LA, LB, LC, LD>(a, mode, f32, lane, bb, kb, bbi, kbi, w, bra, m, p0, q0, s_bra, jj, act,
-                                         sboys);
+            quartet_step<LA, LB, LC, LD, true>(a, mode, f32, lane, bb, kb, bbi, kbi, w, bra, m, p0, q0, s_bra, jj,
+                                               act, sboys);
         }
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, bool EXT>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) quartet_kernel(const FockArgs a, const int mode)
 {
-    quartet_body<LA, LB, LC, LD>(a, mode);
+    quartet_body<LA, LB, LC, LD, EXT>(a, mode);
 }
 
-template <int MB, int LA, int LB, int LC, int LD>
+template <int MB, int LA, int LB, int LC, int LD, bool EXT>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock, MB) quartet_kernel_mb(const FockArgs a, const int mode)
 {
-    quartet_body<LA, LB, LC, LD>(a, mode);
+    quartet_body<LA, LB, LC, LD, EXT>(a, mode);
 }
 
 // the kernel variant of a class
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, bool EXT>
 constexpr auto quartet_kernel_of()
 {
     constexpr int mb = BlocksHint<LA, LB, LC, LD>::value;
     if constexpr (mb > 0)
-        return &quartet_kernel_mb<(mb > 0 ? mb : 1), LA, LB, LC, LD>;
+        return &quartet_kernel_mb<(mb > 0 ? mb : 1), LA, LB, LC, LD, EXT>;
     else
-        return &quartet_kernel<LA, LB, LC, LD>;
+        return &quartet_kernel<LA, LB, LC, LD, EXT>;
+}
+
+// whether a launch needs the extended kernel (density screening,
+// multi-density digestion or quartet counters)
+__host__ __device__ __forceinline__ bool needs_ext(const FockArgs& a)
+{
+    return a.dsh != nullptr || a.dens.n > 0 || a.qstat != nullptr;
 }
 
 // max over all spherical components of (ab|ab) per pair (T4CScreener::partition)

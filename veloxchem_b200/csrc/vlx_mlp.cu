@@ -1,14 +1,16 @@
 // Kernels of the learned initial-guess network: a multilayer perceptron over
 // atom-pair descriptors whose outputs are density-matrix blocks.  Training
 // runs in FP32 (forward with the pre-activations kept, backward, masked mean
-// squared error, Adam); inference can read BF16 weights and BF16-rounded
-// inputs with FP32 accumulation.  The layer shapes are small (inputs of a few
-// dozen features, width 128, outputs up to 196), so each layer is one tiled
-// FP32 GEMM launch with bias and SiLU fused into its epilogue; the same kernel
-// serves the three products of the backward pass through operand strides.
+// squared error, Adam); inference reads BF16 weights and BF16-rounded inputs
+// on the tensor cores (mma.sync, FP32 accumulation).  The layer shapes are
+// small (inputs of about a hundred features, width 128, outputs up to 196),
+// so each layer is one tiled GEMM launch with bias and SiLU fused into its
+// epilogue; the FP32 kernel serves the forward pass of training and the three
+// products of the backward pass through operand strides.
 // No counterpart in the reference (its initial guesses are SAD / core / read).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include <string>
 
@@ -84,6 +86,87 @@ __global__ void __launch_bounds__(256) gemm_kernel(const float* __restrict__ A, 
             Y[(size_t)m * N + n] = act ? silu(z) : z;
         }
     }
+}
+
+// Inference layer on the tensor cores: Y[M, N] = act(X[M, K] W[N, K]^T + b)
+// with X rounded to BF16 as it is staged, W in BF16, FP32 accumulation
+// (mma.sync m16n8k16 BF16, operand fragments read straight from shared
+// memory).  Block: 4 warps on a 64 x 64 output tile, each warp 32 x 32
+// (2 x 4 MMA tiles); K in steps of 16, zero-padded at the edges.
+constexpr int kMmaTile = 64;
+constexpr int kMmaK = 16;
+constexpr int kMmaPad = kMmaK + 8;  // row stride 48 B: the fragment loads of a warp hit 32 distinct banks
+
+__device__ __forceinline__ void mma_bf16_16816(float* c, const uint32_t* a, const uint32_t* b)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) gemm_bf16_mma_kernel(const float* __restrict__ X,
+                                                            const __nv_bfloat16* __restrict__ W,
+                                                            const float* __restrict__ bias, float* __restrict__ Y,
+                                                            const int M, const int N, const int K, const int act)
+{
+    __shared__ __align__(16) __nv_bfloat16 As[kMmaTile][kMmaPad];
+    __shared__ __align__(16) __nv_bfloat16 Bs[kMmaTile][kMmaPad];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    const int m0 = blockIdx.y * kMmaTile, n0 = blockIdx.x * kMmaTile;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+    for (int k0 = 0; k0 < K; k0 += kMmaK) {
+        for (int t = threadIdx.x; t < kMmaTile * kMmaK; t += blockDim.x) {
+            const int r = t / kMmaK, kk = t % kMmaK, k = k0 + kk;
+            const int m = m0 + r, n = n0 + r;
+            As[r][kk] = (m < M && k < K) ? __float2bfloat16_rn(__ldg(X + (size_t)m * K + k)) : zero;
+            Bs[r][kk] = (n < N && k < K) ? W[(size_t)n * K + k] : zero;
+        }
+        __syncthreads();
+        uint32_t a[2][4], b[4][2];
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int r = wm + i * 16 + g;
+            a[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][2 * tq]);
+            a[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * tq]);
+            a[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][2 * tq + 8]);
+            a[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * tq + 8]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int c = wn + j * 8 + g;
+            b[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[c][2 * tq]);
+            b[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[c][2 * tq + 8]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) mma_bf16_16816(acc[i][j], a[i], b[j]);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int m = m0 + wm + i * 16 + g + ((e & 2) ? 8 : 0);
+                const int n = n0 + wn + j * 8 + 2 * tq + (e & 1);
+                if (m < M && n < N) {
+                    const float z = acc[i][j][e] + (bias ? __ldg(bias + n) : 0.0f);
+                    Y[(size_t)m * N + n] = act ? silu(z) : z;
+                }
+            }
 }
 
 // dZ = dY * SiLU'(Z), SiLU'(z) = s (1 + z (1 - s)), s = 1 / (1 + e^-z)
@@ -189,9 +272,9 @@ int vlx_b200_mlp_linear_bf16(const float* X, const void* W_bf16, const float* b,
     if (!X || !W_bf16 || !Y || M < 0 || K < 1 || N < 1)
         return vlx_b200_set_error_internal(VLX_B200_ERR_ARGUMENT, "mlp_linear_bf16: bad arguments");
     if (M == 0) return VLX_B200_OK;
-    const dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
-    gemm_kernel<__nv_bfloat16><<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        X, K, 1, static_cast<const __nv_bfloat16*>(W_bf16), 1, K, b, nullptr, Y, M, N, K, silu_act, 1);
+    const dim3 grid((N + kMmaTile - 1) / kMmaTile, (M + kMmaTile - 1) / kMmaTile);
+    gemm_bf16_mma_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        X, static_cast<const __nv_bfloat16*>(W_bf16), b, Y, M, N, K, silu_act);
     MLP_CHECK();
     return VLX_B200_OK;
 }

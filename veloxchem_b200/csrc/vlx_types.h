@@ -63,6 +63,16 @@ struct MolDev {
     int nl[VLX_LMAX + 1];     // shells per angular momentum (AO stride of component m)
 };
 
+// Densities digested in one pass (multi-density builds): every evaluated
+// quartet is digested into each (D, F) with its own label weights.
+constexpr int kMaxDens = 8;
+struct DensSet {
+    int n;                      // 0: the single density of FockArgs::mol / mols
+    const double* D[kMaxDens];
+    double* F[kMaxDens];
+    double cj[kMaxDens], ck[kMaxDens];
+};
+
 struct FockArgs {
     const PairBlockDev* blocks;
     const WorkItem* items;
@@ -85,6 +95,7 @@ struct FockArgs {
     int nsh;
     float tau_skip, tau32;
     unsigned long long* qstat;  // [2] quartets and primitive quartets evaluated by the launch (nullptr: off)
+    DensSet dens;             // multi-density build (dens.n > 0; single molecule, no density screening)
 };
 
 }  // namespace vlx

@@ -19,7 +19,8 @@ scfrestdriver.py) for the parts a restricted HF energy needs:
   e_en = 2 sum D V (scfdriver.py:2115-2171), F = F_2e + T + V
   (scfdriver.py:2173-2215), electronic gradient
   2 ||X^T (F D S - S D F) X|| (scfrestdriver.py:70-107), Pulay DIIS on the
-  commutator (the reference uses C2-DIIS, c2diis.py), MOs from X^T F X and
+  commutator or the reference's C2-DIIS (``acc_type``, c2diis.py), MOs from
+  X^T F X and
   D = C_occ C_occ^T (scfrestdriver.py:214-269);
 * convergence when the electronic gradient is below ``conv_thresh``
   (default 1e-6, scfdriver.py:151);
@@ -117,6 +118,11 @@ class ScfRestrictedDriver:
         self.conv_thresh = 1.0e-6
         self.max_iter = 50
         self.max_err_vecs = 10
+        # convergence accelerator: 'diis' (Pulay: least-squares weights of the
+        # commutators under sum 1) or 'c2diis' (the reference's CTwoDiis,
+        # c2diis.py:45-243: Sellers' C2-DIIS, the normalised eigenvector of the
+        # error overlap matrix with the smallest residual)
+        self.acc_type = 'diis'
         self.eri_thresh = 1.0e-12
         self.ovl_thresh = 1.0e-6
         self.guess = 'sad'
@@ -151,6 +157,11 @@ class ScfRestrictedDriver:
         self.incremental = True
         self.rebuild_every = 8
         self.inc_skip_factor = 1.0e-2
+        # density-weighted screening of the full builds (the confirmation
+        # build excepted): a quartet is skipped when its bound with the local
+        # maxima of |D| is below full_skip_factor times the dynamic threshold
+        # (0: the reference's Schwarz screening alone)
+        self.full_skip_factor = 0.0
         self.history = []
         self.timings = {}
 
@@ -239,12 +250,15 @@ class ScfRestrictedDriver:
             dl = torch.from_numpy(D_l).to(dev)
             dl = 0.5 * (dl + dl.T).contiguous()
             fl = torch.empty_like(dl)
-            screener.set_density_screening(self._fp32_cutoff(self.early_ithreshold is not None), 0.0)
+            screener.set_density_screening(self._fp32_cutoff(self.early_ithreshold is not None),
+                                           self.full_skip_factor * 10.0 ** (-ith0))
             build(dl, fl, ith0)
             ds = 0.5 * (D + D.T).contiguous()
             fs = torch.empty_like(ds)
-            screener.set_density_screening(1.0e-4, 0.0)
-            build(ds, fs, min(ith0, 6))
+            # the SAD energy only ranks the candidates (their energies differ
+            # by far more than this loose build's error)
+            screener.set_density_screening(1.0e-3, 1.0e-8)
+            build(ds, fs, min(ith0, 5))
             screener.set_density_screening(0.0, 0.0)
             e_l = float(torch.sum(dl * fl) + 2.0 * torch.sum(dl * H))
             e_s = float(torch.sum(ds * fs) + 2.0 * torch.sum(ds * H))
@@ -300,7 +314,7 @@ class ScfRestrictedDriver:
                 F2e.copy_(F2e_prev)
                 F2e.add_(G)
             else:
-                screener.set_density_screening(cutoff, 0.0)
+                screener.set_density_screening(cutoff, self.full_skip_factor * 10.0 ** (-ith))
                 build(D, F2e, ith)
                 ith_used = ith
             torch.cuda.synchronize(dev)
@@ -336,7 +350,10 @@ class ScfRestrictedDriver:
             if len(focks) > self.max_err_vecs:
                 focks.pop(0)
                 errs.pop(0)
-            F_eff = self._diis(focks, errs) if len(focks) > 1 else F
+            if len(focks) > 1:
+                F_eff = self._c2diis(focks, errs) if self.acc_type == 'c2diis' else self._diis(focks, errs)
+            else:
+                F_eff = F
             t0 = time.perf_counter()
             e, c = torch.linalg.eigh(X.T @ F_eff @ X)
             C = X @ c[:, :nocc]
@@ -354,6 +371,36 @@ class ScfRestrictedDriver:
                 'C_alpha': (X @ c).cpu().numpy(), 'E_alpha': e.cpu().numpy(), 'F_alpha': F.cpu().numpy(),
                 'history': self.history, 'timings': dict(self.timings), 'screener': screener,
                 'guess_used': self.guess_used}
+
+    @staticmethod
+    def _c2diis(focks, errs):
+        """C2-DIIS (H. Sellers, Int. J. Quantum Chem. 45, 31 (1993)): the
+        eigenvectors of B_ij = <e_i, e_j>, each rescaled to unit sum (those
+        whose sum is below 1e-6 are dropped), and the one whose combination of
+        error vectors has the smallest norm gives the Fock weights."""
+        torch = _torch()
+        n = len(focks)
+        B = torch.empty((n, n), dtype=torch.float64, device=focks[0].device)
+        for i in range(n):
+            for j in range(i, n):
+                B[i, j] = B[j, i] = torch.sum(errs[i] * errs[j])
+        _, vecs = torch.linalg.eigh(B.cpu())
+        best, best_res = None, None
+        for k in range(n):
+            v = vecs[:, k]
+            s = float(v.sum())
+            if abs(s) <= 1.0e-6:
+                continue
+            w = v / s
+            res = float(w @ B.cpu() @ w)
+            if best_res is None or res < best_res:
+                best, best_res = w, res
+        if best is None:
+            return focks[-1]
+        out = torch.zeros_like(focks[0])
+        for i in range(n):
+            out += float(best[i]) * focks[i]
+        return out
 
     @staticmethod
     def _diis(focks, errs):

@@ -3,6 +3,8 @@
     python -m veloxchem_b200.workloads c3 [--out FILE]     # (H2O)64 / def2-TZVP builds and SCF
     python -m veloxchem_b200.workloads c4 [--out FILE]     # 256 small clusters, batched builds
     python -m veloxchem_b200.workloads c2scf [--out FILE]  # (H2O)32 / def2-SVP SCF, plain and mixed
+    python -m veloxchem_b200.workloads c3h / c4h           # the north-star comparison (bench.py's north_star)
+    python -m veloxchem_b200.workloads build|onee|guess --cluster NAME [--basis B] [--repeat N]
 
 Each prints one JSON object (and writes it to --out).  Times are CUDA-event
 device times for builds and wall-clock times for SCF runs (which include the
@@ -229,7 +231,8 @@ def _time_to(history, e_ref, tol=1e-6):
     return None
 
 
-def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf=True, log=None):
+def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf=True, log=None,
+                full_skip_factor=1e-2):
     """The north-star comparison on (H2O)64 / def2-TZVP in one process:
 
     * builds: the plain FP64 2J-K build (device ms, CUDA events, best of 2
@@ -291,6 +294,8 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
             drv.incremental = inc
             drv.early_ithreshold = early
             drv.conv_thresh = conv
+            if inc:
+                drv.full_skip_factor = full_skip_factor
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
@@ -299,6 +304,7 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
             t_conv6 = next((h['time_s'] for h in hist if h['e_grad'] < 1e-6 and not h.get('mixed')), None)
             runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'], 'converged': res['converged'],
                           'conv_thresh': conv, 'wall_s': wall, 'fock_s': res['timings']['fock_ms_total'] / 1e3,
+                          'timings': {k: v for k, v in res['timings'].items() if isinstance(v, float)},
                           'time_to_grad_1e-6_s': t_conv6, 'guess_used': res['guess_used'], '_history': hist}
             say('c3 scf %s: %d it, %.1f s' % (name, res['iterations'], wall))
         e_ref = runs['plain_fp64_sad']['energy']
@@ -306,6 +312,10 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
             hist = r.pop('_history')
             r['energy_error'] = r['energy'] - e_ref
             r['time_to_1e-6_Eh_s'] = _time_to(hist, e_ref)
+            # per iteration: time (s), |E - E_ref|, gradient, ithreshold, incremental, mixed
+            r['history'] = [[round(h['time_s'], 3), float('%.3g' % abs(h['energy'] - e_ref)),
+                             float('%.3g' % h['e_grad']), h['ithreshold'], int(h['incremental']),
+                             int(h['mixed'])] for h in hist]
         out['scf'] = runs
         out['scf_reference_energy'] = e_ref
         p, m = runs['plain_fp64_sad'], runs['mixed_learned_incremental_early']
@@ -327,9 +337,43 @@ def c4_headline(count=256, nmax=16, reps=3):
             'max_abs_error_vs_single': r['max_abs_error_vs_single']}
 
 
+def onee(cluster, basis, repeat=1):
+    """Overlap, kinetic and nuclear-attraction matrices of a named cluster
+    (the SCF's one-electron integrals), `repeat` times; wall seconds each."""
+    from . import _native as nat
+    mol, bas = _cluster(cluster, basis)
+    times = []
+    for _ in range(repeat):
+        t0 = time.perf_counter()
+        for which in range(3):
+            nat.one_electron(which, mol, bas)
+        times.append(time.perf_counter() - t0)
+    return {'workload': '%s / %s S, T, V' % (cluster, basis), 'nao': bas.get_dimensions_of_basis(), 'seconds': times}
+
+
+def guess(cluster, repeat=1):
+    """Learned-guess inference (descriptors, BF16 network on the tensor
+    cores, assembly, idempotent projection) for a named def2-SVP cluster."""
+    from . import _native as nat
+    from .guess import learned_guess_driver
+    from .scf import SadGuessDriver
+    from . import MolecularBasis
+    mol, bas = _cluster(cluster, 'def2-svp')
+    S = nat.one_electron(0, mol, bas)
+    sad = SadGuessDriver().compute(mol, MolecularBasis.read(mol, 'ao-start-guess'), bas, overlap=S)
+    drv = learned_guess_driver()
+    nocc = mol.number_of_electrons() // 2
+    times = []
+    for _ in range(repeat):
+        t0 = time.perf_counter()
+        drv.predict(mol, bas, sad, S, nocc)
+        times.append(time.perf_counter() - t0)
+    return {'workload': '%s / def2-SVP learned guess' % cluster, 'seconds': times}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build', 'c3h', 'c4h'])
+    ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build', 'c3h', 'c4h', 'onee', 'guess'])
     ap.add_argument('--out', default=None)
     ap.add_argument('--no-scf', action='store_true')
     ap.add_argument('--cluster', default='h2o64')
@@ -343,9 +387,14 @@ def main(argv=None):
         res = build(a.cluster, a.basis, a.repeat, a.fp32_cutoff)
     elif a.which == 'c3h':
         import sys
-        res = c3_headline(scf=not a.no_scf, log=lambda m: print(m, file=sys.stderr, flush=True))
+        res = c3_headline(cutoffs=(1e-5,) if a.no_builds else (1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=not a.no_scf,
+                          log=lambda m: print(m, file=sys.stderr, flush=True))
     elif a.which == 'c4h':
         res = c4_headline()
+    elif a.which == 'onee':
+        res = onee(a.cluster, a.basis, a.repeat)
+    elif a.which == 'guess':
+        res = guess(a.cluster, a.repeat)
     else:
         res = (c3(scf=not a.no_scf, variants=a.scf_variants.split(',') if a.scf_variants else None,
                   builds=not a.no_builds) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf()))
