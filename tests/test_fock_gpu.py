@@ -294,8 +294,7 @@ def test_mixed_precision_build():
         prof = nat.fock_profile(s, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
         n32 = sum(p['fp32_quartets'] for p in prof)
         assert n32 > 0
-        if cutoff >= 1e-7:  # both kernel families evaluate FP32 quartets
-            assert any(p['fp32_quartets'] > 0 for p in prof if p['table_driven'])
+        if cutoff >= 1e-7:
             assert any(p['fp32_quartets'] > 0 for p in prof if not p['table_driven'])
         errors[cutoff] = float((fm - f64).abs().max())
     assert errors[1e-9] < 1e-10 and errors[1e-7] < 1e-8 and errors[1e-5] < 1e-6
@@ -303,6 +302,26 @@ def test_mixed_precision_build():
     f2 = torch.empty_like(d)
     nat.fock_profile(s, d.data_ptr(), f2.data_ptr(), '2jk', 1.0, 12)
     assert float((f2 - f64).abs().max()) < 1e-12
+
+
+def test_mixed_precision_warp_cooperative_classes():
+    """The FP32 twin of the warp-cooperative kernel (the f classes that stay
+    interpreted, present in the def2-TZVP water dimer): FP32 quartets are
+    evaluated there and the Fock error stays below a tenth of the cutoff."""
+    import torch
+    from veloxchem_b200 import _native as nat
+    g, mol, bas = load_golden('h2o_dimer_tzvp.npz')
+    s = _screener(mol, bas)
+    d = torch.from_numpy(g['density']).cuda()
+    f64 = torch.empty_like(d)
+    prof64 = nat.fock_profile(s, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
+    assert any(p['table_driven'] for p in prof64)
+    s.set_fp32_threshold(1e-5, float(d.abs().max()))
+    fm = torch.empty_like(d)
+    prof = nat.fock_profile(s, d.data_ptr(), fm.data_ptr(), '2jk', 1.0, 12)
+    s.set_fp32_threshold(0.0, 0.0)
+    assert any(p['fp32_quartets'] > 0 for p in prof if p['table_driven'])
+    assert float((fm - f64).abs().max()) < 1e-6
 
 
 def test_density_screening_build():

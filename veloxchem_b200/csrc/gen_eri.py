@@ -662,7 +662,9 @@ ACC_COMPILED_MAX = 180
 # with the number of accumulator groups of ClassGen.emit: measured faster
 # than the warp-cooperative kernel on the (H2O)64 / def2-TZVP build.
 GROUPED = {(1, 3, 1, 1): 1, (1, 3, 0, 3): 1, (3, 3, 0, 1): 1, (2, 2, 1, 1): 1, (2, 2, 0, 2): 1, (2, 3, 0, 2): 1,
-           (1, 2, 1, 2): 1, (2, 2, 0, 3): 1, (1, 3, 1, 2): 3, (2, 3, 1, 1): 2}
+           (1, 2, 1, 2): 1, (2, 2, 0, 3): 1, (1, 3, 1, 2): 3, (2, 3, 1, 1): 2,
+           (1, 3, 1, 3): 5, (2, 3, 1, 3): 8, (2, 3, 0, 3): 4, (2, 3, 1, 2): 5, (3, 3, 1, 1): 5, (3, 3, 0, 2): 3,
+           (2, 2, 1, 2): 4, (1, 3, 2, 2): 6, (2, 2, 2, 2): 7, (3, 3, 1, 2): 8, (3, 3, 0, 3): 5}
 
 
 def class_parts(cls):

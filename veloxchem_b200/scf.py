@@ -162,6 +162,9 @@ class ScfRestrictedDriver:
         # maxima of |D| is below full_skip_factor times the dynamic threshold
         # (0: the reference's Schwarz screening alone)
         self.full_skip_factor = 0.0
+        # the same two factors during the early (looser-threshold) iterations,
+        # whose Fock matrices the switch back to the dynamic threshold replaces
+        self.early_skip_factor = None  # None: inc_skip_factor / full_skip_factor
         self.history = []
         self.timings = {}
 
@@ -179,6 +182,9 @@ class ScfRestrictedDriver:
     def _ithreshold(self, e_grad, early):
         ith = int(-math.log10(self.dyn_threshold(e_grad)))
         return min(ith, int(self.early_ithreshold)) if early else ith
+
+    def _skip_factor(self, early, factor):
+        return self.early_skip_factor if (early and self.early_skip_factor is not None) else factor
 
     def _fp32_cutoff(self, early):
         if self.fp32_cutoff <= 0.0:
@@ -251,7 +257,8 @@ class ScfRestrictedDriver:
             dl = 0.5 * (dl + dl.T).contiguous()
             fl = torch.empty_like(dl)
             screener.set_density_screening(self._fp32_cutoff(self.early_ithreshold is not None),
-                                           self.full_skip_factor * 10.0 ** (-ith0))
+                                           self._skip_factor(self.early_ithreshold is not None, self.full_skip_factor)
+                                           * 10.0 ** (-ith0))
             build(dl, fl, ith0)
             ds = 0.5 * (D + D.T).contiguous()
             fs = torch.empty_like(ds)
@@ -308,13 +315,13 @@ class ScfRestrictedDriver:
                 # the FP32 error of an incremental build scales with |dD|, so
                 # its small quartets stay FP32 until convergence
                 screener.set_density_screening(self._fp32_cutoff(early) if self.fp32_cutoff > 0.0 else 0.0,
-                                               self.inc_skip_factor * 10.0 ** (-ith))
+                                               self._skip_factor(early, self.inc_skip_factor) * 10.0 ** (-ith))
                 build(dD, G, ith)
                 ith_used = ith
                 F2e.copy_(F2e_prev)
                 F2e.add_(G)
             else:
-                screener.set_density_screening(cutoff, self.full_skip_factor * 10.0 ** (-ith))
+                screener.set_density_screening(cutoff, self._skip_factor(early, self.full_skip_factor) * 10.0 ** (-ith))
                 build(D, F2e, ith)
                 ith_used = ith
             torch.cuda.synchronize(dev)

@@ -31,8 +31,10 @@ def _cluster(name, basis):
     return mol, MolecularBasis.read(mol, basis)
 
 
-def _build_ms(scr, d, f, reps=3):
-    """Device time (ms, best of reps) of one 2J-K build at ithreshold 12."""
+def _build_ms(scr, d, f, reps=3, enqueue=None):
+    """Device time (ms, best of reps) of one 2J-K build at ithreshold 12;
+    enqueue (a list) receives the host time of each call, which returns once
+    all the build's launches are enqueued."""
     import ctypes
     from . import _native as nat
     torch = _torch()
@@ -42,9 +44,12 @@ def _build_ms(scr, d, f, reps=3):
         for _ in range(reps + 1):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
+            t0 = time.perf_counter()
             nat.check(nat.lib().vlx_b200_fock_build_device(scr.handle, ctypes.c_void_p(d.data_ptr()), 1, b'2jk', 1.0,
                                                             0.0, 12, ctypes.c_void_p(f.data_ptr()),
                                                             ctypes.c_void_p(st.cuda_stream)), 'fock_build')
+            if enqueue is not None:
+                enqueue.append(1e3 * (time.perf_counter() - t0))
             e1.record(st)
             st.synchronize()
             best = min(best, e0.elapsed_time(e1))
@@ -182,26 +187,42 @@ def c4(count=256, nmax=16, reps=5):
     return res
 
 
-def c2scf():
+def c2scf(conv=1e-8):
+    """(H2O)32 / def2-SVP RHF from SAD to an electronic gradient (DIIS error)
+    of `conv`: plain FP64 with Pulay DIIS and with the reference's C2-DIIS,
+    then the mixed / incremental / early variants (Pulay); per run the
+    iterations, wall time, Fock-build time, iterations to a 1e-6 gradient and
+    the energy error against the plain run."""
     from .scf import ScfRestrictedDriver
     mol, bas = _cluster('h2o32', 'def2-svp')
     runs = {}
-    for name, cut, inc, early in (('warmup', 0.0, False, None), ('plain_fp64', 0.0, False, None),
-                                  ('mixed_1e-6', 1e-6, False, None), ('fp64_incremental', 0.0, True, None),
-                                  ('mixed_incremental', 1e-6, True, None), ('mixed_incremental_early8', 1e-6, True, 8)):
+    for name, cut, inc, early, acc in (('warmup', 0.0, False, None, 'diis'),
+                                       ('plain_fp64', 0.0, False, None, 'diis'),
+                                       ('plain_fp64_c2diis', 0.0, False, None, 'c2diis'),
+                                       ('mixed_1e-5', 1e-5, False, None, 'diis'),
+                                       ('fp64_incremental', 0.0, True, None, 'diis'),
+                                       ('mixed_incremental', 1e-5, True, None, 'diis'),
+                                       ('mixed_incremental_early8', 1e-5, True, 8, 'diis')):
         drv = ScfRestrictedDriver()
+        drv.conv_thresh = conv
+        drv.max_iter = 80
         drv.fp32_cutoff = cut
         drv.incremental = inc
         drv.early_ithreshold = early
+        drv.acc_type = acc
+        if inc:
+            drv.full_skip_factor = 1e-2
         t0 = time.perf_counter()
         res = drv.compute(mol, bas)
         if name == 'warmup':
             continue
-        runs[name] = {'energy': res['scf_energy'], 'iterations': res['iterations'],
+        hist = res['history']
+        runs[name] = {'energy': res['scf_energy'], 'converged': res['converged'], 'iterations': res['iterations'],
+                      'iterations_to_grad_1e-6': next((h['iteration'] for h in hist if h['e_grad'] < 1e-6), None),
                       'wall_s': time.perf_counter() - t0, 'fock_ms_total': res['timings']['fock_ms_total']}
-    for k in ('mixed_1e-6', 'fp64_incremental', 'mixed_incremental', 'mixed_incremental_early8'):
+    for k in runs:
         runs[k]['energy_error'] = runs[k]['energy'] - runs['plain_fp64']['energy']
-    return {'workload': '(H2O)32 / def2-SVP RHF from SAD, gradient < 1e-6', **runs}
+    return {'workload': '(H2O)32 / def2-SVP RHF from SAD, electronic gradient < %g' % conv, **runs}
 
 
 def build(cluster, basis, repeat=1, fp32_cutoff=0.0):
@@ -231,8 +252,19 @@ def _time_to(history, e_ref, tol=1e-6):
     return None
 
 
-def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf=True, log=None,
-                full_skip_factor=1e-2):
+def _warm_learned_guess():
+    """Loads the shipped guess network and runs one inference on (H2O)_2."""
+    from . import _native as nat
+    from . import MolecularBasis
+    from .geometry import water_cluster
+    from .guess import learned_guess_driver
+    mol = water_cluster((2, 1, 1), 3)
+    bas = MolecularBasis.read(mol, 'def2-tzvp')
+    learned_guess_driver().predict_any(mol, bas, nat.one_electron(0, mol, bas), mol.number_of_electrons() // 2)
+
+
+def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5, 1e-4), max_fock_error=1e-6, scf=True, log=None,
+                full_skip_factor=1e-2, early_skip_factor=1e-1, fp32_cutoff=1e-4, acc_type='diis'):
     """The north-star comparison on (H2O)64 / def2-TZVP in one process:
 
     * builds: the plain FP64 2J-K build (device ms, CUDA events, best of 2
@@ -241,9 +273,11 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
       is the fastest one whose Fock error stays within ``max_fock_error``;
     * SCF: plain (FP64 full builds every iteration, SAD guess, electronic
       gradient 1e-6, whose final energy E_ref is the FP64 reference: the
-      energy error at that gradient is far below 1e-9 Eh) against mixed +
-      learned + incremental + early iterations (gradient 1e-6), back to back
-      on one screener; per run the wall time to
+      energy error at that gradient is far below 1e-9 Eh) against mixed
+      (FP32 below fp32_cutoff while the gradient is above 1e-4, and in the
+      incremental builds) + learned + incremental + early iterations with
+      per-quartet density screening (gradient 1e-6), back to back on one
+      screener, both with the accelerator acc_type; per run the wall time to
       |E - E_ref| < 1e-6 Eh for good, the time to its declared convergence,
       iterations and the final energy error."""
     from . import T4CScreener
@@ -260,10 +294,15 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
            'screener_s': time.perf_counter() - t0}
     d = torch.from_numpy(random_density(scr.nao, 320, 1)).cuda()
     f64 = torch.empty_like(d)
-    t64 = _build_ms(scr, d, f64, reps=2)
+    enq = []
+    t64 = _build_ms(scr, d, f64, reps=2, enqueue=enq)
     prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
     flops = sum(p['flops'] for p in prof)
     out['fp64_build_ms'] = t64
+    # host time to enqueue one build (work list cached): the launch overhead a
+    # CUDA graph of the build would remove
+    out['enqueue_ms'] = min(enq[1:]) if len(enq) > 1 else None
+    out['kernel_launches_per_build'] = len(prof) + 1  # class kernels + symmetrisation
     out['fp64_tflops'] = flops / t64 / 1e9
     say('c3 fp64 build %.1f ms' % t64)
     dmax = float(d.abs().max())
@@ -284,9 +323,12 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
     out['mixed_sweep'] = sweep
     out['mixed_chosen'] = best
     if scf:
+        # the guess network is loaded (weights, first inference) once per
+        # process, like the library itself, before either timed run
+        _warm_learned_guess()
         runs = {}
         for name, cut, guess, inc, early, conv in (('plain_fp64_sad', 0.0, 'sad', False, None, 1e-6),
-                                                  ('mixed_learned_incremental_early', best['cutoff'], 'learned',
+                                                  ('mixed_learned_incremental_early', fp32_cutoff, 'learned',
                                                    True, 8, 1e-6)):
             drv = ScfRestrictedDriver()
             drv.fp32_cutoff = cut
@@ -294,8 +336,10 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
             drv.incremental = inc
             drv.early_ithreshold = early
             drv.conv_thresh = conv
+            drv.acc_type = acc_type
             if inc:
                 drv.full_skip_factor = full_skip_factor
+                drv.early_skip_factor = early_skip_factor
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
@@ -323,6 +367,47 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), max_fock_error=1e-6, scf
                                               if p['time_to_1e-6_Eh_s'] and m['time_to_1e-6_Eh_s'] else None)
         out['scf_speedup_to_declared_convergence'] = (p['time_to_grad_1e-6_s'] / m['wall_s']
                                                       if p['time_to_grad_1e-6_s'] else None)
+    return out
+
+
+def c3scf_variants(variants, log=None):
+    """(H2O)64 / def2-TZVP SCF: the plain FP64 run (E_ref, gradient 1e-6) and
+    fast variants given as dicts of ScfRestrictedDriver attributes on top of
+    mixed 1e-4 + learned + incremental + early 8 with per-quartet density
+    screening (full skip 1e-2, early skip 1e-1); per run the time to
+    |E - E_ref| < 1e-6 Eh for good, the wall time and the energy error."""
+    from . import T4CScreener
+    from .geometry import random_density
+    from .scf import ScfRestrictedDriver
+    torch = _torch()
+    say = log or (lambda *a: None)
+    mol, bas = _cluster('h2o64', 'def2-tzvp')
+    scr = T4CScreener()
+    scr.partition(bas, mol, 'eri')
+    d = torch.from_numpy(random_density(scr.nao, 320, 1)).cuda()
+    _build_ms(scr, d, torch.empty_like(d), reps=0)  # work list of threshold 12
+    base = dict(fp32_cutoff=1e-4, guess='learned', incremental=True, early_ithreshold=8, full_skip_factor=1e-2,
+                early_skip_factor=1e-1)
+    out = {}
+    for name, attrs in [('plain', dict(fp32_cutoff=0.0, guess='sad', incremental=False))] + list(variants):
+        drv = ScfRestrictedDriver()
+        for k, v in (attrs if name == 'plain' else {**base, **attrs}).items():
+            setattr(drv, k, v)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = drv.compute(mol, bas, screener=scr)
+        out[name] = {'attrs': attrs, 'wall_s': time.perf_counter() - t0, 'energy': res['scf_energy'],
+                     'iterations': res['iterations'], '_h': res['history']}
+        say('%s: %d it, %.1f s' % (name, res['iterations'], out[name]['wall_s']))
+    e_ref = out['plain']['energy']
+    for r in out.values():
+        h = r.pop('_h')
+        r['energy_error'] = r['energy'] - e_ref
+        r['time_to_1e-6_Eh_s'] = _time_to(h, e_ref)
+        r['history'] = [[round(x['time_s'], 3), float('%.3g' % abs(x['energy'] - e_ref)), x['ithreshold'],
+                         int(x['incremental'])] for x in h]
+    for r in out.values():
+        r['speedup'] = (out['plain']['time_to_1e-6_Eh_s'] / r['time_to_1e-6_Eh_s']) if r['time_to_1e-6_Eh_s'] else None
     return out
 
 
@@ -373,7 +458,7 @@ def guess(cluster, repeat=1):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build', 'c3h', 'c4h', 'onee', 'guess'])
+    ap.add_argument('which', choices=['c3', 'c4', 'c2scf', 'build', 'c3h', 'c4h', 'c3scf', 'onee', 'guess'])
     ap.add_argument('--out', default=None)
     ap.add_argument('--no-scf', action='store_true')
     ap.add_argument('--cluster', default='h2o64')
@@ -391,6 +476,15 @@ def main(argv=None):
                           log=lambda m: print(m, file=sys.stderr, flush=True))
     elif a.which == 'c4h':
         res = c4_headline()
+    elif a.which == 'c3scf':
+        import sys
+        _warm_learned_guess()
+        res = c3scf_variants([('fast', {}),
+                              ('plain_c2diis', dict(fp32_cutoff=0.0, guess='sad', incremental=False,
+                                                    early_ithreshold=None, acc_type='c2diis')),
+                              ('fast_c2diis', dict(acc_type='c2diis')),
+                              ('fast_again', {})],
+                             log=lambda m: print(m, file=sys.stderr, flush=True))
     elif a.which == 'onee':
         res = onee(a.cluster, a.basis, a.repeat)
     elif a.which == 'guess':
