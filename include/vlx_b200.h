@@ -222,6 +222,17 @@ int vlx_b200_set_fp32_threshold(vlx_b200_screener* screener, double cutoff, doub
  * Schwarz bins only, T4CScreener / BlockedGtoPairBlock). */
 int vlx_b200_set_density_screening(vlx_b200_screener* screener, double fp32_cutoff, double skip_cutoff);
 
+/* For the following density-screened builds with an FP32 cutoff: on != 0
+ * digests the FP32 quartets of the compiled classes in FP32 (an FP32 copy of
+ * D, a separate FP32 accumulator added to the FP64 result at the end), which
+ * halves their digestion bytes; 0 (the default) digests them in FP64.  Each
+ * FP32 contribution is below the FP32 cutoff, but the FP32 sums carry a
+ * rounding error that grows with the number of contributions per element
+ * ((H2O)64 / def2-TZVP at cutoff 1e-4: enough to hold an SCF 3e-7 Eh off), so
+ * it suits builds whose result is replaced later, such as the early, looser
+ * iterations of an SCF.  No counterpart in the reference. */
+int vlx_b200_set_fp32_digestion(vlx_b200_screener* screener, int on);
+
 /* Dense (nao)^4 ERI tensor over the screened unique quartets (all eight
  * index permutations written), host buffer.
  * Replaces CFockDriver::compute_eri(screener, nao, ithreshold)

@@ -357,6 +357,15 @@ def test_density_screening_build():
               % (cutoff, n32, nqm, n32_bins, err))
         assert nqm == nq and n32 > 0
         assert err < 0.1 * cutoff
+    # FP32 digestion of the FP32 quartets (FP32 copy of D, FP32 accumulator)
+    s.set_fp32_digestion(True)
+    for cutoff in (1e-7, 1e-5):
+        s.set_density_screening(cutoff, 0.0)
+        fd, nqd, n32 = build(d)
+        err = float((fd - f64).abs().max())
+        print('density screening fp32 cutoff %.0e with FP32 digestion: error %.2e' % (cutoff, err))
+        assert nqd == nq and n32 > 0 and err < 0.1 * cutoff
+    s.set_fp32_digestion(False)
     for skip in (1e-12, 1e-10):
         s.set_density_screening(0.0, skip)
         fs, nqs, _ = build(d)

@@ -52,6 +52,7 @@ SIGNATURES = {
                                              _ip, _ip, _ip, _dp, _dp, ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]),
     'vlx_b200_set_fp32_threshold': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     'vlx_b200_set_density_screening': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    'vlx_b200_set_fp32_digestion': (ctypes.c_int, [_vp, ctypes.c_int]),
     'vlx_b200_fock_build_noalloc': (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_int, _vp, _vp]),
     'vlx_b200_mlp_linear': (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -34,11 +34,17 @@ def nvcc():
     return exe
 
 
-def _headers_digest():
+def _headers_digest(abi=False):
+    """Digest of the headers a unit may include: the device headers for every
+    unit, plus the public C header (abi=True) for the units that include it
+    (the host orchestration and the guess-network kernels; the per-class
+    units do not)."""
     h = hashlib.sha256()
-    for p in sorted(list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) +
-                    [GEN / 'dispatch.inc', GEN / 'sph_table.inc', GEN / 'xform.inc', GEN / 'coop_classes.inc',
-                     INCLUDE / 'vlx_b200.h']):
+    files = list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h')) + \
+        [GEN / 'dispatch.inc', GEN / 'sph_table.inc', GEN / 'xform.inc', GEN / 'coop_classes.inc']
+    if abi:
+        files.append(INCLUDE / 'vlx_b200.h')
+    for p in sorted(files):
         if p.exists():
             h.update(p.read_bytes())
     h.update(' '.join(NVCC_FLAGS).encode())
@@ -75,13 +81,17 @@ def build(jobs=None, lmax=3, verbose=True):
                 '    .byte 0\n    .section .note.GNU-stack,"",@progbits\n' % blob)
     if not asm.exists() or asm.read_text() != asm_text:
         asm.write_text(asm_text)
-    hdr = _headers_digest()
+    hdr, hdr_abi = _headers_digest(), _headers_digest(abi=True)
+    abi_units = {'vlx_host', 'vlx_mlp', 'vlx_onee', 'vlx_coop'}
     sources = sorted(GEN.glob('class_*.cu')) + [CSRC / 'vlx_coop.cu', CSRC / 'vlx_onee.cu', CSRC / 'vlx_mlp.cu',
                                                 CSRC / 'vlx_host.cu']
     objs = [OBJ / (s.stem + '.o') for s in sources]
     jobs = jobs or os.cpu_count() or 4
+    # the longest units first, so that they do not finish last on one core
+    order = sorted(range(len(sources)), key=lambda k: -sources[k].stat().st_size)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        futs = [ex.submit(_compile, s, o, hdr) for s, o in zip(sources, objs)]
+        futs = [ex.submit(_compile, sources[k], objs[k], hdr_abi if sources[k].stem in abi_units else hdr)
+                for k in order]
         for f in cf.as_completed(futs):
             name, dt, built = f.result()
             if verbose and built:

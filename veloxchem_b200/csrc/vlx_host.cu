@@ -234,19 +234,46 @@ int device_globals(int device, DeviceGlobals** out)
 }
 
 // ------------------------------------------------------------------ kernels local to the host TU
-__global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ out, const int n)
+// out = A + A^T with A = acc (+ acc32, the FP32 accumulator of a
+// density-screened build, when given), 32 x 32 tiles through shared memory.
+__global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ out, const int n,
+                                  const float* __restrict__ acc32 = nullptr)
 {
     __shared__ double tile[32][33];
     const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x;
     for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
         const int r = bx * 32 + ty, c = by * 32 + tx;
-        tile[ty][tx] = (r < n && c < n) ? acc[(size_t)r * n + c] : 0.0;
+        double v = 0.0;
+        if (r < n && c < n) {
+            v = acc[(size_t)r * n + c];
+            if (acc32) v += (double)acc32[(size_t)r * n + c];
+        }
+        tile[ty][tx] = v;
     }
     __syncthreads();
     for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
         const int i = by * 32 + ty, j = bx * 32 + tx;
-        if (i < n && j < n) out[(size_t)i * n + j] = acc[(size_t)i * n + j] + tile[tx][ty];
+        if (i < n && j < n) {
+            double v = acc[(size_t)i * n + j] + tile[tx][ty];
+            if (acc32) v += (double)acc32[(size_t)i * n + j];
+            out[(size_t)i * n + j] = v;
+        }
     }
+}
+
+// out = acc + acc32 (general densities with an FP32 accumulator)
+__global__ void add_acc32_kernel(const double* __restrict__ acc, const float* __restrict__ acc32,
+                                 double* __restrict__ out, const size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = acc[i] + (double)acc32[i];
+}
+
+// D rounded to float (the FP32 digestion's copy of the density)
+__global__ void to_float_kernel(const double* __restrict__ x, float* __restrict__ y, const size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
 }
 
 // Shell-block maxima of |D| for per-quartet density screening: dsh[A nsh + B]
@@ -372,12 +399,15 @@ struct vlx_b200_screener {
     int part = 0;       // rank/nodes partition of later builds: 0 round-robin (reference), 1 cost-balanced
     // per-quartet density screening of later builds (vlx_b200_set_density_screening; 0: off)
     double dscr_fp32 = 0.0, dscr_skip = 0.0;
+    bool fp32_digest = false;    // FP32 quartets of density-screened builds digest in FP32 (set_fp32_digestion)
     float* d_dsh = nullptr;      // nsh x nsh shell-block max |D| of the build's density
     int2* d_shinfo = nullptr;    // per shell: AO index of component 0, angular momentum
     unsigned long long* d_qstat = nullptr;  // profiled builds: [class][FP64, FP32][quartets, primitive quartets]
     int nqstat = 0;
     double* d_multi = nullptr;  // multi-density builds: densities / outputs, then accumulators
     int nmulti = 0;
+    float* d_D32 = nullptr;     // density-screened builds: D rounded to float, FP32 accumulator
+    float* d_F32 = nullptr;
     std::vector<TaskSet> tasksets;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -738,6 +768,8 @@ struct LaunchCtx {
     float tau_skip = 0.0f, tau32 = 0.0f;
     unsigned long long* qstat = nullptr;  // [class][FP64, FP32][2] quartet counters (profiled builds)
     vlx::DensSet dens{};                  // multi-density build (dens.n > 0)
+    const float* D32 = nullptr;           // FP32 digestion of the FP32 quartets (density-screened builds)
+    float* F32 = nullptr;
 };
 
 // Enqueues all class kernels of a task set on `st`; the accumulators must be
@@ -767,6 +799,8 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.dsh = L.dsh;
     a.nsh = L.nsh;
     a.dens = L.dens;
+    a.D32 = L.D32;
+    a.F32 = L.F32;
     a.tau_skip = L.tau_skip;
     a.tau32 = L.tau32;
     const int nprec = (L.dsh ? L.tau32 > 0.0f : ith32 >= 0) ? 2 : 1;
@@ -823,11 +857,14 @@ int prepare_dscr(vlx_b200_screener* s, const double* dD, cudaStream_t st)
     return VLX_B200_OK;
 }
 
+// acc32 (out, may be null): the FP32 accumulator the build used, which the
+// symmetrisation must add (nullptr: none).
 int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* dD, double* dAcc, double* eri,
                     double cj, double ck, double omega2, int ith, int ith32, cudaStream_t st, long long* launches,
                     std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* events = nullptr,
-                    unsigned long long* qstat = nullptr)
+                    unsigned long long* qstat = nullptr, const float** acc32 = nullptr)
 {
+    if (acc32) *acc32 = nullptr;
     LaunchCtx L;
     L.blocks = s->d_blocks;
     L.glob = s->glob;
@@ -845,6 +882,21 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
         L.nsh = (int)s->shells.size();
         L.tau_skip = (float)s->dscr_skip;
         L.tau32 = (float)s->dscr_fp32;
+        if (s->dscr_fp32 > 0.0 && s->fp32_digest && acc32) {
+            // the FP32 quartets digest in FP32 into their own accumulator
+            const size_t nn = (size_t)s->nao * s->nao;
+            if (!s->d_D32) {
+                VLX_CUDA(cudaMalloc(&s->d_D32, std::max<size_t>(nn, 1) * sizeof(float)));
+                VLX_CUDA(cudaMalloc(&s->d_F32, std::max<size_t>(nn, 1) * sizeof(float)));
+            }
+            to_float_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(dD, s->d_D32, nn);
+            VLX_CUDA(cudaGetLastError());
+            VLX_CUDA(cudaMemsetAsync(s->d_F32, 0, nn * sizeof(float), st));
+            if (launches) (*launches)++;
+            L.D32 = s->d_D32;
+            L.F32 = s->d_F32;
+            *acc32 = s->d_F32;
+        }
     }
     return enqueue_ctx(L, ts, mode, eri, cj, ck, omega2, ith, ith32, st, launches, events);
 }
@@ -906,12 +958,13 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
     if (rc) return rc;
     const size_t bytes = (size_t)s->nao * s->nao * sizeof(double);
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
+    const float* acc32 = nullptr;
     if (known) {
         TaskSet* ts = nullptr;
         rc = build_tasks(s, ith, rank, nodes, &ts);
         if (rc) return rc;
         rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dD, s->d_acc, nullptr, cj,
-                             ck, omega2, ith, s->ith32, st, launches);
+                             ck, omega2, ith, s->ith32, st, launches, nullptr, nullptr, &acc32);
         if (rc) return rc;
         if (quartets || prim) {
             long long q = ts->quartets, pq = ts->prim_quartets;
@@ -930,7 +983,12 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
     }
     if (symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, dF, s->nao);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, dF, s->nao, acc32);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    } else if (acc32) {
+        const size_t nn = (size_t)s->nao * s->nao;
+        add_acc32_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(s->d_acc, acc32, dF, nn);
         VLX_CUDA(cudaGetLastError());
         if (launches) (*launches)++;
     } else {
@@ -1135,6 +1193,8 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_shinfo) cudaFree(s->d_shinfo);
     if (s->d_qstat) cudaFree(s->d_qstat);
     if (s->d_multi) cudaFree(s->d_multi);
+    if (s->d_D32) cudaFree(s->d_D32);
+    if (s->d_F32) cudaFree(s->d_F32);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1234,6 +1294,8 @@ int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int nde
     const int chunk = std::min(ndens, vlx::kMaxDens);
     if (s->nmulti < chunk) {
         if (s->d_multi) cudaFree(s->d_multi);
+    if (s->d_D32) cudaFree(s->d_D32);
+    if (s->d_F32) cudaFree(s->d_F32);
         s->d_multi = nullptr;
         VLX_CUDA(cudaMalloc(&s->d_multi, 2 * (size_t)chunk * std::max<size_t>(bytes, 8)));
         s->nmulti = chunk;
@@ -1547,6 +1609,13 @@ int vlx_b200_set_density_screening(vlx_b200_screener* s, double fp32_cutoff, dou
     return VLX_B200_OK;
 }
 
+int vlx_b200_set_fp32_digestion(vlx_b200_screener* s, int on)
+{
+    if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
+    s->fp32_digest = on != 0;
+    return VLX_B200_OK;
+}
+
 int vlx_b200_set_fp32_threshold(vlx_b200_screener* s, double cutoff, double max_abs_density)
 {
     if (!s) return fail(VLX_B200_ERR_ARGUMENT, "null screener");
@@ -1617,17 +1686,24 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     if (dev_count && s->nqstat < (int)(4 * nc)) {
         if (s->d_qstat) cudaFree(s->d_qstat);
     if (s->d_multi) cudaFree(s->d_multi);
+    if (s->d_D32) cudaFree(s->d_D32);
+    if (s->d_F32) cudaFree(s->d_F32);
         s->d_qstat = nullptr;
         s->nqstat = std::max<int>(4 * (int)nc, 256);
         VLX_CUDA(cudaMalloc(&s->d_qstat, s->nqstat * sizeof(unsigned long long)));
     }
     if (dev_count) VLX_CUDA(cudaMemsetAsync(s->d_qstat, 0, 4 * nc * sizeof(unsigned long long), st));
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
+    const float* acc32 = nullptr;
     rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, dev_count ? s->d_qstat : nullptr);
+                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, dev_count ? s->d_qstat : nullptr, &acc32);
     if (!rc && symmetric) {
         const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao, acc32);
+    } else if (!rc && acc32) {
+        const size_t nn = (size_t)s->nao * s->nao;
+        add_acc32_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(s->d_acc, acc32, d_fock,
+                                                                                             nn);
     } else if (!rc) {
         cudaMemcpyAsync(d_fock, s->d_acc, bytes, cudaMemcpyDeviceToDevice, st);
     }

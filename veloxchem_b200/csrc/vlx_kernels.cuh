@@ -9,19 +9,22 @@
 
 namespace vlx {
 
-__device__ __forceinline__ double warp_sum(double v)
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-__device__ __forceinline__ double ldD(const double* __restrict__ D, int nao, int r, int c)
+template <typename T>
+__device__ __forceinline__ T ldD(const T* __restrict__ D, int nao, int r, int c)
 {
     return __ldg(D + (size_t)r * nao + c);
 }
 
-__device__ __forceinline__ void addF(double* F, int nao, int r, int c, double v)
+template <typename T>
+__device__ __forceinline__ void addF(T* F, int nao, int r, int c, T v)
 {
     atomicAdd(F + (size_t)r * nao + c, v);
 }
@@ -31,27 +34,27 @@ __device__ __forceinline__ void addF(double* F, int nao, int r, int c, double v)
 // (1/2 for P == Q, 1/2 for R == S, 1/2 for PQ == RS) and is 0 on idle lanes.
 // Symmetric density (reference local_distribute_rest_*): contributions are
 // accumulated in one orientation and the caller adds the transpose at the end.
-template <int NA, int NB, int NC, int ND, int MODE>
-__device__ __forceinline__ void digest(const double* f, const double s, const int lane, const int p0, const int nlp,
-                                       const int q0, const int nlq, const int r0, const int nlr, const int s0,
-                                       const int nls, const MolDev& m, const double cjw, const double ckw)
+// T = double, or float for the FP32 digestion of FP32 quartets into the
+// separate FP32 accumulator of a density-screened build (FP32 copy of D).
+template <int NA, int NB, int NC, int ND, int MODE, typename T>
+__device__ __forceinline__ void digest_t(const T* f, const T s, const int lane, const int p0, const int nlp,
+                                         const int q0, const int nlq, const int r0, const int nlr, const int s0,
+                                         const int nls, const T* __restrict__ D, T* F, const int nao, const T cjw,
+                                         const T ckw)
 {
-    const double* __restrict__ D = m.D;
-    double* F = m.F;
-    const int nao = m.nao;
-    const double cj = cjw * s, ck = ckw * s;
-    if (cjw != 0.0) {
+    const T cj = cjw * s, ck = ckw * s;
+    if (cjw != T(0)) {
         // F_PQ: reduce over the lanes (ket pairs), then one atomic per element
 #pragma unroll
         for (int i = 0; i < NA; i++) {
 #pragma unroll
             for (int j = 0; j < NB; j++) {
-                double v = 0.0;
+                T v = T(0);
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
 #pragma unroll
                     for (int l = 0; l < ND; l++) {
-                        double d = ldD(D, nao, r0 + k * nlr, s0 + l * nls);
+                        T d = ldD(D, nao, r0 + k * nlr, s0 + l * nls);
                         if (MODE == MODE_FOCK_GEN) d += ldD(D, nao, s0 + l * nls, r0 + k * nlr);
                         v = fma(f[((i * NB + j) * NC + k) * ND + l], d, v);
                     }
@@ -64,17 +67,17 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
             }
         }
         // F_RS: per lane
-        if (s != 0.0) {
+        if (s != T(0)) {
 #pragma unroll
             for (int k = 0; k < NC; k++) {
 #pragma unroll
                 for (int l = 0; l < ND; l++) {
-                    double v = 0.0;
+                    T v = T(0);
 #pragma unroll
                     for (int i = 0; i < NA; i++) {
 #pragma unroll
                         for (int j = 0; j < NB; j++) {
-                            double d = ldD(D, nao, p0 + i * nlp, q0 + j * nlq);
+                            T d = ldD(D, nao, p0 + i * nlp, q0 + j * nlq);
                             if (MODE == MODE_FOCK_GEN) d += ldD(D, nao, q0 + j * nlq, p0 + i * nlp);
                             v = fma(f[((i * NB + j) * NC + k) * ND + l], d, v);
                         }
@@ -85,18 +88,18 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
             }
         }
     }
-    if (ckw != 0.0 && s != 0.0) {
+    if (ckw != T(0) && s != T(0)) {
         // F_PR += sum_{j l} f D_QS ; F_RP (general) += sum f D_SQ
 #pragma unroll
         for (int i = 0; i < NA; i++) {
 #pragma unroll
             for (int k = 0; k < NC; k++) {
-                double v = 0.0, w = 0.0;
+                T v = T(0), w = T(0);
 #pragma unroll
                 for (int j = 0; j < NB; j++) {
 #pragma unroll
                     for (int l = 0; l < ND; l++) {
-                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        const T x = f[((i * NB + j) * NC + k) * ND + l];
                         v = fma(x, ldD(D, nao, q0 + j * nlq, s0 + l * nls), v);
                         if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, s0 + l * nls, q0 + j * nlq), w);
                     }
@@ -110,12 +113,12 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
         for (int i = 0; i < NA; i++) {
 #pragma unroll
             for (int l = 0; l < ND; l++) {
-                double v = 0.0, w = 0.0;
+                T v = T(0), w = T(0);
 #pragma unroll
                 for (int j = 0; j < NB; j++) {
 #pragma unroll
                     for (int k = 0; k < NC; k++) {
-                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        const T x = f[((i * NB + j) * NC + k) * ND + l];
                         v = fma(x, ldD(D, nao, q0 + j * nlq, r0 + k * nlr), v);
                         if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, r0 + k * nlr, q0 + j * nlq), w);
                     }
@@ -129,12 +132,12 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
         for (int j = 0; j < NB; j++) {
 #pragma unroll
             for (int k = 0; k < NC; k++) {
-                double v = 0.0, w = 0.0;
+                T v = T(0), w = T(0);
 #pragma unroll
                 for (int i = 0; i < NA; i++) {
 #pragma unroll
                     for (int l = 0; l < ND; l++) {
-                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        const T x = f[((i * NB + j) * NC + k) * ND + l];
                         v = fma(x, ldD(D, nao, p0 + i * nlp, s0 + l * nls), v);
                         if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, s0 + l * nls, p0 + i * nlp), w);
                     }
@@ -148,12 +151,12 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
         for (int j = 0; j < NB; j++) {
 #pragma unroll
             for (int l = 0; l < ND; l++) {
-                double v = 0.0, w = 0.0;
+                T v = T(0), w = T(0);
 #pragma unroll
                 for (int i = 0; i < NA; i++) {
 #pragma unroll
                     for (int k = 0; k < NC; k++) {
-                        const double x = f[((i * NB + j) * NC + k) * ND + l];
+                        const T x = f[((i * NB + j) * NC + k) * ND + l];
                         v = fma(x, ldD(D, nao, p0 + i * nlp, r0 + k * nlr), v);
                         if (MODE == MODE_FOCK_GEN) w = fma(x, ldD(D, nao, r0 + k * nlr, p0 + i * nlp), w);
                     }
@@ -163,6 +166,14 @@ __device__ __forceinline__ void digest(const double* f, const double s, const in
             }
         }
     }
+}
+
+template <int NA, int NB, int NC, int ND, int MODE>
+__device__ __forceinline__ void digest(const double* f, const double s, const int lane, const int p0, const int nlp,
+                                       const int q0, const int nlq, const int r0, const int nlr, const int s0,
+                                       const int nls, const MolDev& m, const double cjw, const double ckw)
+{
+    digest_t<NA, NB, NC, ND, MODE, double>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m.D, m.F, m.nao, cjw, ckw);
 }
 
 // Scatter one unique spherical quartet into the dense ERI tensor (all eight
@@ -265,6 +276,24 @@ __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, 
         } else {
             const PairViewF braf = make_view_f(bb, w.bra, bra.kuse);
             C::compute_f32(braf, ketf, reinterpret_cast<const float*>(sboys), (float)a.omega2, g);
+        }
+        if constexpr (EXT) {
+            // density-screened build with an FP32 accumulator: the FP32
+            // quartets (each contribution below the FP32 cutoff) are digested
+            // in FP32 against the FP32 copy of D
+            if (a.F32 != nullptr && (mode & 3) != MODE_ERI) {
+                const int r0 = __ldg(kb.ao + jj), s0 = __ldg(kb.ao + kb.npairs + jj);
+                float s = act ? (float)s_bra : 0.0f;
+                if (r0 == s0) s *= 0.5f;
+                if (bbi == kbi && jj == w.bra) s *= 0.5f;
+                if ((mode & 3) == MODE_FOCK_SYM)
+                    digest_t<NA, NB, NC, ND, MODE_FOCK_SYM, float>(g, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls,
+                                                                   a.D32, a.F32, m.nao, (float)a.cj, (float)a.ck);
+                else
+                    digest_t<NA, NB, NC, ND, MODE_FOCK_GEN, float>(g, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls,
+                                                                   a.D32, a.F32, m.nao, (float)a.cj, (float)a.ck);
+                return;
+            }
         }
 #pragma unroll
         for (int t = 0; t < C::NSPH; t++) f[t] = (double)g[t];

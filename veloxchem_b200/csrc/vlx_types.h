@@ -102,6 +102,12 @@ struct FockArgs {
     float tau_skip, tau32;
     unsigned long long* qstat;  // [2] quartets and primitive quartets evaluated by the launch (nullptr: off)
     DensSet dens;             // multi-density build (dens.n > 0; single molecule, no density screening)
+    // density-screened builds: the FP32 quartets of the compiled classes are
+    // digested in FP32 against D32 (D rounded to float) into the FP32
+    // accumulator F32, added to the FP64 result by the symmetrisation
+    // (nullptr: FP32 quartets digest in FP64)
+    const float* D32;
+    float* F32;
 };
 
 }  // namespace vlx

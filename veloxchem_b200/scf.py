@@ -165,6 +165,9 @@ class ScfRestrictedDriver:
         # the same two factors during the early (looser-threshold) iterations,
         # whose Fock matrices the switch back to the dynamic threshold replaces
         self.early_skip_factor = None  # None: inc_skip_factor / full_skip_factor
+        # the early builds' FP32 quartets digest in FP32 (their Fock matrices
+        # are replaced by the switch build); the later builds digest in FP64
+        self.early_fp32_digestion = True
         self.history = []
         self.timings = {}
 
@@ -256,6 +259,7 @@ class ScfRestrictedDriver:
             dl = torch.from_numpy(D_l).to(dev)
             dl = 0.5 * (dl + dl.T).contiguous()
             fl = torch.empty_like(dl)
+            screener.set_fp32_digestion(self.early_ithreshold is not None and self.early_fp32_digestion)
             screener.set_density_screening(self._fp32_cutoff(self.early_ithreshold is not None),
                                            self._skip_factor(self.early_ithreshold is not None, self.full_skip_factor)
                                            * 10.0 ** (-ith0))
@@ -300,6 +304,7 @@ class ScfRestrictedDriver:
                 focks.clear()
                 errs.clear()
             ith = self._ithreshold(e_grad, early)
+            screener.set_fp32_digestion(early and self.early_fp32_digestion)
             D = 0.5 * (D + D.T).contiguous()
             mixed = self.fp32_cutoff > 0.0 and e_grad > self.fp32_until_grad
             cutoff = self._fp32_cutoff(early) if mixed else 0.0
@@ -347,7 +352,12 @@ class ScfRestrictedDriver:
                                      'ithreshold': ith, 'mixed': False, 'incremental': False, 'check': True,
                                      'time_s': time.perf_counter() - t_start})
                 if e_grad >= self.conv_thresh:
+                    # the incremental Fock matrices carried an error the full
+                    # build removed: continue with full builds and a fresh
+                    # DIIS subspace
                     incremental = False
+                    focks.clear()
+                    errs.clear()
             if e_grad < self.conv_thresh and not early:
                 converged = True
                 break
@@ -368,6 +378,7 @@ class ScfRestrictedDriver:
             torch.cuda.synchronize(dev)
             eigh_s += time.perf_counter() - t0
         screener.set_density_screening(0.0, 0.0)
+        screener.set_fp32_digestion(False)
         self.timings['fock_ms_total'] = fock_ms
         self.timings['diag_s'] = eigh_s
         self.timings['total_s'] = time.perf_counter() - t_start

@@ -121,6 +121,11 @@ class T4CScreener:
         nat.check(nat.lib().vlx_b200_set_density_screening(self.handle, float(fp32_cutoff), float(skip_cutoff)),
                   'set_density_screening')
 
+    def set_fp32_digestion(self, on):
+        """FP32 digestion of the FP32 quartets of density-screened builds
+        (for builds whose result is replaced later: see the C header)."""
+        nat.check(nat.lib().vlx_b200_set_fp32_digestion(self.handle, int(bool(on))), 'set_fp32_digestion')
+
     def set_work_threshold(self, ithreshold_base):
         """Build work lists for max(ithreshold, ithreshold_base) and filter at
         run time, so builds at several thresholds share one list."""
