@@ -344,15 +344,19 @@ int vlx_b200_to_bf16(const float* x, void* y_bf16, long long n, void* stream);
  * is one global knob: CFockDriver::set_block_size_factor,
  * src/t4c_func/FockDriver.cpp:356-404).  Times every quartet class of a
  * 2J-K build of d_density at `ithreshold` under several ket-run lengths per
- * work item and keeps the fastest per class for the screener's later builds
- * (all thresholds); synchronises `stream`.  Results are numerically the same
+ * work item, then, with the chosen lengths, the compiled classes under caps
+ * of 1, 2 and 4 resident blocks per SM, and keeps the fastest choice per
+ * class for the screener's later builds (all thresholds); synchronises
+ * `stream`.  Results are numerically the same
  * builds (only the order of the FP64 atomic additions changes). */
 typedef struct {
     int la, lb, lc, ld;
     int table_driven;   /* 1: warp-cooperative kernel */
     int segment;        /* chosen ket pairs per work item */
-    double best_ms;     /* device time of the class with the chosen length */
-    double default_ms;  /* ... with the default length */
+    double best_ms;     /* device time of the class with the chosen length and cap */
+    double default_ms;  /* ... with the default length, uncapped */
+    int blocks_per_sm;  /* chosen cap of resident blocks per SM of the class's persistent
+                           launch (compiled classes; 0: the occupancy limit) */
 } vlx_b200_tune_result;
 
 int vlx_b200_autotune(vlx_b200_screener* screener, const double* d_density, int ithreshold, void* stream,

@@ -88,7 +88,7 @@ class ClassProfile(ctypes.Structure):
 class TuneResult(ctypes.Structure):
     _fields_ = [('la', ctypes.c_int), ('lb', ctypes.c_int), ('lc', ctypes.c_int), ('ld', ctypes.c_int),
                 ('table_driven', ctypes.c_int), ('segment', ctypes.c_int), ('best_ms', ctypes.c_double),
-                ('default_ms', ctypes.c_double)]
+                ('default_ms', ctypes.c_double), ('blocks_per_sm', ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -392,6 +392,10 @@ struct vlx_b200_screener {
     int seg = 256;
     // autotuned ket-run length per quartet class (key la | lb << 4 | lc << 8 | ld << 12)
     std::map<int, int> class_seg;
+    // autotuned cap of resident blocks per SM of a compiled class's persistent
+    // launch (same key; absent: the occupancy limit)
+    std::map<int, int> class_bps;
+    int bps_try = 0;                           // cap being timed while tuning (0: off)
     int tune_gen = 0;                          // bumped whenever class_seg changes (task-set cache key)
     int seg_try_compiled = 0, seg_try_coop = 0;  // candidate lengths while tuning (0: off)
     int ith32 = -1;  // mixed precision: quartets with bin sum >= ith32 in FP32 (-1: off)
@@ -770,6 +774,8 @@ struct LaunchCtx {
     vlx::DensSet dens{};                  // multi-density build (dens.n > 0)
     const float* D32 = nullptr;           // FP32 digestion of the FP32 quartets (density-screened builds)
     float* F32 = nullptr;
+    const std::map<int, int>* bps = nullptr;  // per-class caps of resident blocks per SM (compiled classes)
+    int bps_try = 0;                          // a cap for every compiled class (autotuning; 0: off)
 };
 
 // Enqueues all class kernels of a task set on `st`; the accumulators must be
@@ -819,7 +825,13 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
             const int fmode = f ? (mode | vlx::MODE_F32) : mode;
             if (ct.compiled >= 0) {
                 const auto& e = vlx::kQuartetClasses[ct.compiled];
-                const int occ = std::max(1, e.occupancy(vlx::needs_ext(af) ? 1 : 0));
+                int occ = std::max(1, e.occupancy(vlx::needs_ext(af) ? 1 : 0));
+                if (L.bps_try > 0) {
+                    occ = std::min(occ, L.bps_try);
+                } else if (L.bps) {
+                    const auto cap = L.bps->find(ct.la | (ct.lb << 4) | (ct.lc << 8) | (ct.ld << 12));
+                    if (cap != L.bps->end()) occ = std::min(occ, cap->second);
+                }
                 const int want = (int)((ct.items.size() + warps_per_block - 1) / warps_per_block);
                 e.launch(fmode, af, std::max(1, std::min(want, occ * nsm)), st);
             } else {
@@ -874,6 +886,8 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     L.mol.nao = s->nao;
     for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
     L.qstat = qstat;
+    L.bps = &s->class_bps;
+    L.bps_try = s->bps_try;
     if (mode != vlx::MODE_ERI && dscr_active(s)) {
         const int rc = prepare_dscr(s, dD, st);
         if (rc) return rc;
@@ -2160,6 +2174,8 @@ struct TuneCandidate {
     int compiled, coop;
 };
 constexpr TuneCandidate kTuneCandidates[] = {{256, 2}, {32, 1}, {64, 2}, {128, 4}, {512, 8}};
+// caps of resident blocks per SM tried for the compiled classes
+constexpr int kTuneBlockCaps[] = {1, 2, 4};
 
 }  // namespace
 
@@ -2227,12 +2243,12 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
             ++it;
         }
     }
-    s->ith32 = ith32_saved;
     if (rc) {
+        s->ith32 = ith32_saved;
         s->tune_gen++;
         return rc;
     }
-    int n = 0;
+    std::map<int, float> best_ms;
     for (const auto& kv : times) {
         const auto& v = kv.second;
         size_t best = 0;
@@ -2240,19 +2256,80 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
             if (v[k] < v[best]) best = k;
         const bool coop = kind[kv.first] != 0;
         s->class_seg[kv.first] = coop ? kTuneCandidates[best].coop : kTuneCandidates[best].compiled;
+        best_ms[kv.first] = v[best];
+    }
+    // second pass, with the chosen lengths: a cap on the resident blocks per
+    // SM of each compiled class's persistent launch (fewer resident threads
+    // keep the thread-local frames of the large classes in L2); a cap is kept
+    // when it beats the uncapped launch by more than 2%
+    s->class_bps.clear();
+    s->tune_gen = gen0 + 1 + (int)ncand;
+    TaskSet* tsb = nullptr;
+    rc = build_tasks(s, ith, 0, 1, &tsb);
+    for (const int cap : kTuneBlockCaps) {
+        if (rc) break;
+        s->bps_try = cap;
+        const size_t nc = tsb->classes.size();
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev(nc);
+        for (auto& e : ev) {
+            VLX_CUDA(cudaEventCreate(&e.first));
+            VLX_CUDA(cudaEventCreate(&e.second));
+        }
+        VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, (size_t)s->nao * s->nao * sizeof(double), st));
+        rc = enqueue_classes(s, tsb, vlx::MODE_FOCK_SYM, d_density, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
+                             nullptr, &ev);
+        const cudaError_t e = cudaStreamSynchronize(st);
+        if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+        for (size_t c = 0; c < nc && !rc; c++) {
+            const ClassTasks& ct = tsb->classes[c];
+            if (ct.items.empty() || ct.compiled < 0) continue;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[c].first, ev[c].second);
+            const int key = ct.la | (ct.lb << 4) | (ct.lc << 8) | (ct.ld << 12);
+            if (ms < 0.98f * best_ms[key]) {
+                best_ms[key] = ms;
+                s->class_bps[key] = cap;
+            }
+        }
+        for (auto& x : ev) {
+            cudaEventDestroy(x.first);
+            cudaEventDestroy(x.second);
+        }
+    }
+    s->bps_try = 0;
+    for (auto it = s->tasksets.begin(); it != s->tasksets.end();) {
+        if (it->tune_gen >= gen0) {
+            if (it->d_items) cudaFree(it->d_items);
+            it = s->tasksets.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    s->ith32 = ith32_saved;
+    if (rc) {
+        s->class_bps.clear();
+        s->tune_gen = gen0 + 2 + (int)ncand;
+        return rc;
+    }
+    int n = 0;
+    for (const auto& kv : times) {
+        const auto& v = kv.second;
         if (n < max_classes) {
             vlx_b200_tune_result& r = out[n++];
             r.la = kv.first & 15;
             r.lb = (kv.first >> 4) & 15;
             r.lc = (kv.first >> 8) & 15;
             r.ld = (kv.first >> 12) & 15;
-            r.table_driven = coop ? 1 : 0;
+            r.table_driven = kind[kv.first] ? 1 : 0;
             r.segment = s->class_seg[kv.first];
-            r.best_ms = v[best];
+            r.best_ms = best_ms[kv.first];
             r.default_ms = v[0];
+            const auto cap = s->class_bps.find(kv.first);
+            r.blocks_per_sm = (cap == s->class_bps.end()) ? 0 : cap->second;
         }
     }
-    s->tune_gen++;
+    // later builds make their work lists with the chosen lengths
+    s->tune_gen = gen0 + 2 + (int)ncand;
     *nclasses = n;
     return VLX_B200_OK;
 }

@@ -56,7 +56,7 @@ def _build_ms(scr, d, f, reps=3, enqueue=None):
     return best
 
 
-def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=True):
+def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=True, autotune=False):
     from . import T4CScreener
     from . import _native as nat
     from .geometry import random_density
@@ -70,6 +70,11 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=T
     out = {'workload': '(H2O)64 / def2-TZVP, 2J-K, ithreshold 12', 'nao': scr.nao}
     if not builds:
         cutoffs = ()
+    if autotune:
+        out['fp64_build_ms_untuned'] = _build_ms(scr, d, torch.empty_like(d), reps=1)
+        t0 = time.perf_counter()
+        out['autotune'] = nat.autotune(scr, d.data_ptr(), 12)
+        out['autotune_s'] = time.perf_counter() - t0
     t64 = _build_ms(scr, d, f64, reps=3 if builds else 0)
     prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
     flops = sum(p['flops'] for p in prof)
@@ -476,6 +481,7 @@ def main(argv=None):
     ap.add_argument('--fp32-cutoff', type=float, default=0.0)
     ap.add_argument('--scf-variants', default=None, help='comma-separated subset of the C3 SCF variants')
     ap.add_argument('--no-builds', action='store_true', help='C3: skip the per-cutoff build table')
+    ap.add_argument('--autotune', action='store_true', help='C3: autotune the classes first')
     a = ap.parse_args(argv)
     if a.which == 'build':
         res = build(a.cluster, a.basis, a.repeat, a.fp32_cutoff)
@@ -499,7 +505,8 @@ def main(argv=None):
         res = guess(a.cluster, a.repeat)
     else:
         res = (c3(scf=not a.no_scf, variants=a.scf_variants.split(',') if a.scf_variants else None,
-                  builds=not a.no_builds) if a.which == 'c3' else (c4() if a.which == 'c4' else c2scf()))
+                  builds=not a.no_builds, autotune=a.autotune) if a.which == 'c3'
+               else (c4() if a.which == 'c4' else c2scf()))
     text = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, 'w') as fh:
