@@ -347,7 +347,9 @@ def run_ours(args):
                                'parallelism': ('one build sharded over %d GPUs (cost-balanced work items, NCCL '
                                                'all-reduce of the FP64 partials)' % world) if world > 1
                                else 'single GPU',
-                               'autotuned_classes': sum(1 for t in tuned if t['best_ms'] < t['default_ms'])}),
+                               'autotuned_classes': sum(1 for t in tuned if t['best_ms'] < t['default_ms']),
+                               'autotune': ['%d%d%d%d:%d/%d' % (t['la'], t['lb'], t['lc'], t['ld'], t['segment'],
+                                                                t['blocks_per_sm']) for t in tuned]}),
             'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e,
             'gpu_launches': launches_per_build * args.steps, 'clocks': clk,
             'quartets_per_build': int(sum(p['shell_quartets'] for p in prof)),

@@ -621,6 +621,10 @@ def emit_class_file(cls, outdir):
     w('// Generated by gen_eri.py -- do not edit.')
     w('#include "vlx_kernels.cuh"')
     w('namespace vlx {')
+    w('template <> struct BlocksHint<%d, %d, %d, %d> { static constexpr int value = %d; };'
+      % (cls + (BLOCKS_HINT.get(tuple(cls), 0),)))
+    w('template <> struct StageBra<%d, %d, %d, %d> { static constexpr bool value = %s; };'
+      % (cls + ('true' if tuple(cls) in STAGE_BRA else 'false',)))
     w(g.emit(parts=class_parts(cls)))
     w('')
     w('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st)' % nm)
@@ -665,6 +669,22 @@ GROUPED = {(1, 3, 1, 1): 1, (1, 3, 0, 3): 1, (3, 3, 0, 1): 1, (2, 2, 1, 1): 1, (
            (1, 2, 1, 2): 1, (2, 2, 0, 3): 1, (1, 3, 1, 2): 3, (2, 3, 1, 1): 2,
            (1, 3, 1, 3): 5, (2, 3, 1, 3): 8, (2, 3, 0, 3): 4, (2, 3, 1, 2): 5, (3, 3, 1, 1): 5, (3, 3, 0, 2): 3,
            (2, 2, 1, 2): 4, (1, 3, 2, 2): 6, (2, 2, 2, 2): 7, (3, 3, 1, 2): 8, (3, 3, 0, 3): 5}
+
+
+# Minimum resident 128-thread blocks per SM a class's register allocation
+# must allow (absent: no minimum).  4 for classes whose unconstrained
+# allocation (164-168 registers, 3 blocks) fits 128 registers without
+# spilling (measured 15-20% faster each); a minimum of 3 for the classes at
+# 250+ registers was measured neutral.  An explicit minimum of 1 is not the
+# same as none: it lets the compiler take far more registers (186 instead of
+# 72 for (sp|ss)).
+BLOCKS_HINT = {(1, 1, 0, 0): 4, (0, 1, 0, 1): 5, (0, 2, 0, 0): 5, (0, 1, 0, 0): 8, (1, 1, 0, 1): 4, (0, 2, 0, 1): 4}
+
+# Classes whose bra primitive records are staged in shared memory per work
+# item: measured faster staged on the (H2O)32 / def2-SVP build ((ss|ss)
+# 1.19x, (sp|ss) 1.08x, (pp|ss) 1.05x, (sd|ss) 1.03x, (dd|pd) 1.46x); the
+# other classes measured neutral to slower (down to 0.34x for (dd|dd)).
+STAGE_BRA = {(0, 0, 0, 0), (0, 1, 0, 0), (1, 1, 0, 0), (0, 2, 0, 0), (2, 2, 1, 2)}
 
 
 def class_parts(cls):

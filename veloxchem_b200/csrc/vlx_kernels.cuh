@@ -203,41 +203,21 @@ __device__ __forceinline__ void scatter_eri(const double* f, const int p0, const
 
 constexpr int kWarpsPerBlock = 4;
 
-// Minimum resident 128-thread blocks per SM a class's register allocation
-// must allow (0: no minimum).  4 for classes whose unconstrained allocation
-// (164-168 registers, 3 blocks) fits 128 registers without spilling (measured:
-// 15-20% faster each); a minimum of 3 for the classes at 250+ registers was
-// measured neutral.  An explicit minimum of 1 is not the same as none: it
-// lets the compiler take far more registers (186 instead of 72 for (sp|ss)).
+// Per-class tuning traits, specialised in each class's generated unit from the
+// tables of gen_eri.py (BLOCKS_HINT, STAGE_BRA), so that tuning one class
+// recompiles only that unit:
+//   BlocksHint::value  minimum resident 128-thread blocks per SM the class's
+//                      register allocation must allow (0: no minimum);
+//   StageBra::value    stage the bra primitive records in shared memory per
+//                      work item (PairViewS).
 template <int LA, int LB, int LC, int LD>
-struct BlocksHint {
-    static constexpr int value = 0;
-};
-template <> struct BlocksHint<1, 1, 0, 0> { static constexpr int value = 4; };
-template <> struct BlocksHint<0, 1, 0, 1> { static constexpr int value = 5; };
-template <> struct BlocksHint<0, 2, 0, 0> { static constexpr int value = 5; };
-template <> struct BlocksHint<0, 1, 0, 0> { static constexpr int value = 8; };
-template <> struct BlocksHint<1, 1, 0, 1> { static constexpr int value = 4; };
-template <> struct BlocksHint<0, 2, 0, 1> { static constexpr int value = 4; };
+struct BlocksHint;
+template <int LA, int LB, int LC, int LD>
+struct StageBra;
 
 // One step of a work item: lane evaluates ket pair jj of kb against the bra
 // pair (act = false: an idle lane, which computes and contributes nothing)
 // and digests the spherical block.
-// Classes whose bra primitive fields are staged in shared memory per work
-// item (PairViewS): chosen by measurement, per class.
-template <int LA, int LB, int LC, int LD>
-struct StageBra {
-    static constexpr bool value = VLX_STAGE_BRA_DEFAULT;
-};
-// measured faster staged on the (H2O)32 / def2-SVP build: (ss|ss) 1.19x,
-// (sp|ss) 1.08x, (pp|ss) 1.05x, (sd|ss) 1.03x, (dd|pd) 1.46x; the other
-// classes measured neutral to slower (down to 0.34x for (dd|dd))
-template <> struct StageBra<0, 0, 0, 0> { static constexpr bool value = true; };
-template <> struct StageBra<0, 1, 0, 0> { static constexpr bool value = true; };
-template <> struct StageBra<1, 1, 0, 0> { static constexpr bool value = true; };
-template <> struct StageBra<0, 2, 0, 0> { static constexpr bool value = true; };
-template <> struct StageBra<2, 2, 1, 2> { static constexpr bool value = true; };
-
 // EXT = false: the plain build (one density, the reference's screening);
 // EXT = true adds the per-quartet density screening, multi-density digestion
 // and the device quartet counters, in a separate instantiation so that the

@@ -22,11 +22,6 @@
 // Highest angular momentum per shell compiled into the class kernels.
 #define VLX_LMAX 3
 
-// Whether the class kernels stage the bra primitive records in shared memory
-// unless a class says otherwise (StageBra in vlx_kernels.cuh).
-#ifndef VLX_STAGE_BRA_DEFAULT
-#define VLX_STAGE_BRA_DEFAULT 0
-#endif
 
 namespace vlx {
 
