@@ -217,11 +217,13 @@ def test_c2diis_weights_find_the_zero_residual_combination():
 
 
 @pytest.mark.gpu
-def test_scf_energy_known_answer_c2diis():
+def test_scf_energy_known_answer_pulay_diis():
+    """The known answer with Pulay DIIS (the driver's default is the
+    reference's C2-DIIS, which the other SCF tests use)."""
     from veloxchem_b200.scf import ScfRestrictedDriver
     mol, bas = _dimer()
     drv = ScfRestrictedDriver()
-    drv.acc_type = 'c2diis'
+    drv.acc_type = 'diis'
     res = drv.compute(mol, bas)
     assert res['converged']
     assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
