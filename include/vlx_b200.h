@@ -169,9 +169,10 @@ int vlx_b200_set_partition(vlx_b200_screener* screener, int mode);
  * framework holding most of HBM, or fixed per-rank pools in an MPI job), or a
  * caller that runs other streams next to the Fock build and cannot afford the
  * device-wide synchronisation that cudaFree implies.  This entry point takes
- * its scratch (the FP64 Fock accumulator and the work-queue heads) from a
- * static device array of the library instead: 8 MiB, held by every GPU that
- * loads the library until the process exits, enough for nao <= 1024.
+ * its scratch (the FP64 Fock accumulator, the density in the library's
+ * internal AO order and the work-queue heads) from static device arrays of
+ * the library instead: 16 MiB, held by every GPU that loads the library until
+ * the process exits, enough for nao <= 1024.
  *
  * d_density / d_fock: device pointers (nao x nao) on the screener's device;
  * stream: cudaStream_t (NULL = the screener's own stream); label, ithreshold,
@@ -185,7 +186,7 @@ int vlx_b200_set_partition(vlx_b200_screener* screener, int mode);
  *    applies as in vlx_b200_fock_build_device;
  *  - the first call on a device looks up the address of the static array on
  *    that device, so make that first call before any stream capture;
- *  - all calls share the one array, which keeps the previous call's contents
+ *  - all calls share the same arrays, which keep the previous call's contents
  *    (each call clears what it needs): calls that overlap on the GPU, from
  *    two streams or two screeners, race and give wrong results. */
 int vlx_b200_fock_build_noalloc(vlx_b200_screener* screener, const double* d_density, int symmetric,

@@ -625,6 +625,8 @@ def emit_class_file(cls, outdir):
       % (cls + (BLOCKS_HINT.get(tuple(cls), 0),)))
     w('template <> struct StageBra<%d, %d, %d, %d> { static constexpr bool value = %s; };'
       % (cls + ('true' if tuple(cls) in STAGE_BRA else 'false',)))
+    w('template <> struct AccumulateJ<%d, %d, %d, %d> { static constexpr int value = %d; };'
+      % (cls + (ACCUM_J.get(tuple(cls), 0),)))
     w(g.emit(parts=class_parts(cls)))
     w('')
     w('void launch_quartet_%s(int mode, const FockArgs& a, int grid, cudaStream_t st)' % nm)
@@ -685,6 +687,16 @@ BLOCKS_HINT = {(1, 1, 0, 0): 4, (0, 1, 0, 1): 5, (0, 2, 0, 0): 5, (0, 1, 0, 0): 
 # 1.19x, (sp|ss) 1.08x, (pp|ss) 1.05x, (sd|ss) 1.03x, (dd|pd) 1.46x); the
 # other classes measured neutral to slower (down to 0.34x for (dd|dd)).
 STAGE_BRA = {(0, 0, 0, 0), (0, 1, 0, 0), (1, 1, 0, 0), (0, 2, 0, 0), (2, 2, 1, 2)}
+
+
+# Classes whose plain kernels sum the J elements of the bra block F_PQ per
+# work item (1: in registers, 2: in a per-warp shared-memory array) instead of
+# one warp sum and atomic add per 32-ket step (absent: per step).  Chosen per
+# class from timings of all three forms on the (H2O)32 / def2-SVP and
+# (H2O)64 / def2-TZVP builds (gains 3-12% per class; (sp|ss), (sp|sp),
+# (ss|ss), (pd|pd), (pd|pp) measured neutral or slower and stay per step).
+ACCUM_J = {(1, 1, 0, 1): 1, (1, 2, 0, 1): 2, (1, 1, 0, 0): 2, (0, 2, 0, 1): 2, (0, 2, 1, 1): 2, (0, 2, 0, 0): 2,
+           (1, 1, 1, 1): 2, (1, 2, 0, 2): 2, (1, 2, 0, 0): 1, (0, 3, 0, 1): 2, (0, 3, 1, 2): 1}
 
 
 def class_parts(cls):

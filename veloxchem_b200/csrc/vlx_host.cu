@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -116,13 +117,26 @@ long double boys_series(int m, long double t)
     return std::exp(-t) * sum;
 }
 
+// Per (order, interval): the Chebyshev interpolant of degree BOYS_NCOEF - 1 at
+// the Chebyshev nodes of the interval's local variable x in [-1, 1], rewritten
+// in the monomial basis of x (T_0 = 1, T_1 = x, T_{j+1} = 2x T_j - T_{j-1}) so
+// that the device evaluates it by Horner's rule.  The coefficients decay fast
+// (|c_9| ~ 1e-17 relative), so the monomial form on [-1, 1] stays as well
+// conditioned as the Chebyshev one.
 std::vector<double> make_boys_table()
 {
     const int N = BOYS_NCOEF;
+    // monomial coefficients of T_0 .. T_{N-1}
+    long double tj[BOYS_NCOEF][BOYS_NCOEF] = {};
+    tj[0][0] = 1.0L;
+    if (N > 1) tj[1][1] = 1.0L;
+    for (int j = 2; j < N; j++)
+        for (int k = 0; k < N; k++)
+            tj[j][k] = (k > 0 ? 2.0L * tj[j - 1][k - 1] : 0.0L) - tj[j - 2][k];
     std::vector<double> tab((size_t)(BOYS_MMAX + 1) * BOYS_NINT * N);
     for (int m = 0; m <= BOYS_MMAX; m++)
         for (int it = 0; it < BOYS_NINT; it++) {
-            long double fv[BOYS_NCOEF];
+            long double fv[BOYS_NCOEF], cheb[BOYS_NCOEF];
             for (int k = 0; k < N; k++) {
                 const long double x = std::cos(M_PI * (k + 0.5L) / N);
                 const long double h = 1.0L / BOYS_INV_H;
@@ -133,7 +147,12 @@ std::vector<double> make_boys_table()
                 for (int k = 0; k < N; k++) s += fv[k] * std::cos(M_PI * j * (k + 0.5L) / N);
                 s *= 2.0L / N;
                 if (j == 0) s *= 0.5L;
-                tab[((size_t)(m * BOYS_NINT + it)) * N + j] = (double)s;
+                cheb[j] = s;
+            }
+            for (int k = 0; k < N; k++) {
+                long double a = 0.0L;
+                for (int j = k; j < N; j++) a += cheb[j] * tj[j][k];
+                tab[((size_t)(m * BOYS_NINT + it)) * N + k] = (double)a;
             }
         }
     return tab;
@@ -235,9 +254,10 @@ int device_globals(int device, DeviceGlobals** out)
 
 // ------------------------------------------------------------------ kernels local to the host TU
 // out = A + A^T with A = acc (+ acc32, the FP32 accumulator of a
-// density-screened build, when given), 32 x 32 tiles through shared memory.
+// density-screened build, when given), 32 x 32 tiles through shared memory;
+// with perm, element (i, j) of the internal order goes to (perm[i], perm[j]).
 __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __restrict__ out, const int n,
-                                  const float* __restrict__ acc32 = nullptr)
+                                  const float* __restrict__ acc32 = nullptr, const int* __restrict__ perm = nullptr)
 {
     __shared__ double tile[32][33];
     const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x;
@@ -256,8 +276,49 @@ __global__ void symmetrize_kernel(const double* __restrict__ acc, double* __rest
         if (i < n && j < n) {
             double v = acc[(size_t)i * n + j] + tile[tx][ty];
             if (acc32) v += (double)acc32[(size_t)i * n + j];
-            out[(size_t)i * n + j] = v;
+            if (perm)
+                out[(size_t)__ldg(perm + i) * n + __ldg(perm + j)] = v;
+            else
+                out[(size_t)i * n + j] = v;
         }
+    }
+}
+
+// Internal order in: dst(i, j) = src(perm[i], perm[j]), one block per row.
+__global__ void permute_in_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                  const int* __restrict__ perm, const int n)
+{
+    const int i = blockIdx.x;
+    const double* row = src + (size_t)__ldg(perm + i) * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) dst[(size_t)i * n + j] = row[__ldg(perm + j)];
+}
+
+// Internal order out (general matrices): dst(perm[i], perm[j]) = acc(i, j)
+// (+ acc32), one block per row.
+__global__ void permute_out_kernel(const double* __restrict__ acc, const float* __restrict__ acc32,
+                                   double* __restrict__ dst, const int* __restrict__ perm, const int n)
+{
+    const int i = blockIdx.x;
+    double* row = dst + (size_t)__ldg(perm + i) * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double v = acc[(size_t)i * n + j];
+        if (acc32) v += (double)acc32[(size_t)i * n + j];
+        row[__ldg(perm + j)] = v;
+    }
+}
+
+// The ERI tensor in the caller's order: dst(perm[p], perm[q], perm[r],
+// perm[s]) = src(p, q, r, s), one block per (p, q).
+__global__ void permute_eri_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                   const int* __restrict__ perm, const int n)
+{
+    const size_t nn = (size_t)n * n;
+    const int p = blockIdx.x / n, q = blockIdx.x % n;
+    const size_t base = ((size_t)__ldg(perm + p) * n + __ldg(perm + q)) * nn;
+    const double* in = src + ((size_t)p * n + q) * nn;
+    for (size_t rs = threadIdx.x; rs < nn; rs += blockDim.x) {
+        const int r = (int)(rs / n), t = (int)(rs % n);
+        dst[base + (size_t)__ldg(perm + r) * n + __ldg(perm + t)] = in[rs];
     }
 }
 
@@ -334,7 +395,9 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b)
 // ------------------------------------------------------------------ screener state
 struct Shell {
     double xyz[3];
-    int l, nprim, ao0;
+    int l, nprim;
+    int ao0;      // internal AO index of component 0 (the kernels' numbering)
+    int ao0_ref;  // the caller's AO index of component 0 (MolecularBasis order)
     std::vector<double> e, c;
 };
 
@@ -345,6 +408,7 @@ struct PairBlock {
     std::vector<int> bin;                    // reference order
     std::vector<int> sorted;                 // sorted position -> reference index (bins >= 0)
     int bin_off[17];                         // sorted pairs with bin < b start at bin_off[b]
+    std::vector<int> nuse_ref;               // reference order: significant primitive pairs
     std::vector<int> nuse;                   // sorted order: significant primitive pairs
     std::vector<long long> nuse_prefix;      // sorted order: prefix sums of nuse
 };
@@ -380,6 +444,12 @@ struct vlx_b200_screener {
     int nao = 0, lmax = 0;
     int nl[VLX_LMAX + 1] = {0};
     std::vector<Shell> shells;
+    // internal AO order (see screener_create): perm[internal AO] = caller's AO;
+    // D is permuted into it and F back out of it at the boundary of a build
+    std::vector<int> perm;
+    bool permuted = false;
+    int* d_perm = nullptr;
+    double* d_Dint = nullptr;  // the build's density in the internal order
     std::vector<PairBlock> blocks;
     std::vector<PairBlockDev> h_blocks;
     PairBlockDev* d_blocks = nullptr;
@@ -446,7 +516,10 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
     s->h_blocks.assign(nb, PairBlockDev{});
     const double kconst = std::sqrt(2.0 / std::sqrt(M_PI));
     for (size_t b = 0; b < nb; b++) {
-        if (sorted) s->blocks[b].nuse.assign(npairs[b], 0);
+        if (sorted)
+            s->blocks[b].nuse.assign(npairs[b], 0);
+        else
+            s->blocks[b].nuse_ref.assign(npairs[b], 0);
         const PairBlock& pb = s->blocks[b];
         const size_t n = npairs[b];
         const int kp = pb.ka * pb.kb;
@@ -502,7 +575,10 @@ int upload_pairs(vlx_b200_screener* s, bool sorted)
             int used = 0;
             while (used < kp && std::fabs(vals[used][2]) >= VLX_PRIM_CUTOFF) used++;
             nuse[i] = std::max(used, 1);
-            if (sorted) s->blocks[b].nuse[i] = nuse[i];
+            if (sorted)
+                s->blocks[b].nuse[i] = nuse[i];
+            else
+                s->blocks[b].nuse_ref[i] = nuse[i];
             for (int p = 0; p < kp; p++)
                 for (int f = 0; f < 9; f++) {
                     prim[((size_t)f * kp + p) * n + i] = vals[p][f];
@@ -754,6 +830,51 @@ int ensure_buffers(vlx_b200_screener* s)
     if (!s->d_acc) VLX_CUDA(cudaMalloc(&s->d_acc, std::max<size_t>(bytes, 8)));
     if (!s->d_D) VLX_CUDA(cudaMalloc(&s->d_D, std::max<size_t>(bytes, 8)));
     if (!s->d_F) VLX_CUDA(cudaMalloc(&s->d_F, std::max<size_t>(bytes, 8)));
+    if (s->permuted && !s->d_Dint) VLX_CUDA(cudaMalloc(&s->d_Dint, std::max<size_t>(bytes, 8)));
+    return VLX_B200_OK;
+}
+
+// The density the class kernels read: the caller's dD (caller's AO order)
+// itself, or its copy in the screener's internal order, written to `buf`
+// (default: the screener's d_Dint, from ensure_buffers).
+int internal_density(vlx_b200_screener* s, const double* dD, cudaStream_t st, const double** out,
+                     long long* launches, double* buf = nullptr)
+{
+    *out = dD;
+    if (!s->permuted) return VLX_B200_OK;
+    double* dst = buf ? buf : s->d_Dint;
+    if (s->nao > 0) {
+        permute_in_kernel<<<s->nao, 256, 0, st>>>(dD, dst, s->d_perm, s->nao);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    }
+    *out = dst;
+    return VLX_B200_OK;
+}
+
+// F in the caller's AO order from the internal accumulator acc (+ acc32, the
+// FP32 accumulator of a density-screened build): A + A^T for symmetric
+// densities, A otherwise.
+int write_fock(const vlx_b200_screener* s, const double* acc, const float* acc32, double* dF, bool symmetric,
+               cudaStream_t st, long long* launches)
+{
+    const int n = s->nao;
+    if (n == 0) return VLX_B200_OK;
+    const size_t nn = (size_t)n * n;
+    const int* perm = s->permuted ? s->d_perm : nullptr;
+    if (symmetric) {
+        const dim3 grid((n + 31) / 32, (n + 31) / 32), blk(32, 8);
+        symmetrize_kernel<<<grid, blk, 0, st>>>(acc, dF, n, acc32, perm);
+    } else if (perm) {
+        permute_out_kernel<<<n, 256, 0, st>>>(acc, acc32, dF, perm, n);
+    } else if (acc32) {
+        add_acc32_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(acc, acc32, dF, nn);
+    } else {
+        VLX_CUDA(cudaMemcpyAsync(dF, acc, nn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return VLX_B200_OK;
+    }
+    VLX_CUDA(cudaGetLastError());
+    if (launches) (*launches)++;
     return VLX_B200_OK;
 }
 
@@ -977,7 +1098,10 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
         TaskSet* ts = nullptr;
         rc = build_tasks(s, ith, rank, nodes, &ts);
         if (rc) return rc;
-        rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dD, s->d_acc, nullptr, cj,
+        const double* dI = nullptr;
+        rc = internal_density(s, dD, st, &dI, launches);
+        if (rc) return rc;
+        rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dI, s->d_acc, nullptr, cj,
                              ck, omega2, ith, s->ith32, st, launches, nullptr, nullptr, &acc32);
         if (rc) return rc;
         if (quartets || prim) {
@@ -995,20 +1119,7 @@ int device_build(vlx_b200_screener* s, int rank, int nodes, const double* dD, in
             if (prim) *prim += pq;
         }
     }
-    if (symmetric) {
-        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, dF, s->nao, acc32);
-        VLX_CUDA(cudaGetLastError());
-        if (launches) (*launches)++;
-    } else if (acc32) {
-        const size_t nn = (size_t)s->nao * s->nao;
-        add_acc32_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(s->d_acc, acc32, dF, nn);
-        VLX_CUDA(cudaGetLastError());
-        if (launches) (*launches)++;
-    } else {
-        VLX_CUDA(cudaMemcpyAsync(dF, s->d_acc, bytes, cudaMemcpyDeviceToDevice, st));
-    }
-    return VLX_B200_OK;
+    return write_fock(s, s->d_acc, acc32, dF, symmetric != 0, st, launches);
 }
 
 int host_build(vlx_b200_screener* s, int rank, int nodes, const double* density, int symmetric, const char* label,
@@ -1124,7 +1235,35 @@ int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, co
     for (auto& sh : s->shells) s->nl[sh.l]++;
     for (int l = 0; l <= VLX_LMAX; l++) loff[l + 1] = loff[l] + s->nl[l] * (2 * l + 1);
     s->nao = loff[VLX_LMAX + 1];
-    for (auto& sh : s->shells) sh.ao0 = loff[sh.l] + cnt[sh.l]++;
+    for (auto& sh : s->shells) sh.ao0_ref = loff[sh.l] + cnt[sh.l]++;
+    // Internal AO numbering: within an angular momentum, the shells of one GTO
+    // block (same contraction depth) are numbered contiguously, in input order.
+    // The ket pairs of a pair block run over consecutive shells of its second
+    // GTO block, so the lanes of one step then read D and add into F at
+    // adjacent columns (shared 32-byte sectors) instead of columns spread by
+    // the other shells of each atom.
+    {
+        std::vector<int> order(s->shells.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [s](int x, int y) {
+            const Shell& a = s->shells[x];
+            const Shell& b = s->shells[y];
+            return a.l != b.l ? a.l < b.l : a.nprim < b.nprim;
+        });
+        int pos[VLX_LMAX + 1] = {0};
+        for (int i : order) {
+            Shell& sh = s->shells[i];
+            sh.ao0 = loff[sh.l] + pos[sh.l]++;
+        }
+        s->perm.assign(s->nao, 0);
+        for (const Shell& sh : s->shells)
+            for (int m = 0; m < 2 * sh.l + 1; m++) s->perm[sh.ao0 + m * s->nl[sh.l]] = sh.ao0_ref + m * s->nl[sh.l];
+        for (int i = 0; i < s->nao; i++) s->permuted = s->permuted || s->perm[i] != i;
+        if (cudaMalloc(&s->d_perm, std::max<size_t>(s->perm.size(), 1) * sizeof(int)) != cudaSuccess ||
+            cudaMemcpy(s->d_perm, s->perm.data(), s->perm.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            return cleanup(fail(VLX_B200_ERR_CUDA, "screener_create: AO permutation upload failed"));
+    }
     // GTO blocks (l ascending, distinct contraction depths ascending)
     std::vector<std::pair<int, int>> gblocks;  // (l, K)
     std::vector<std::vector<int>> gshells;
@@ -1180,10 +1319,19 @@ int vlx_b200_screener_create(vlx_b200_screener** out, int device, int natoms, co
         }
         pb.bin_off[0] = 0;
         for (int k = 0; k < 16; k++) pb.bin_off[k + 1] = pb.bin_off[k] + count[k];
+        // within a bin, pairs with more significant primitive pairs first (the
+        // reference's order among equals): the lanes of one step of a work item
+        // then run about the same number of ket primitives, where the reference
+        // order mixes near pairs (all Ka x Kb primitive pairs) with far pairs
+        // (often a single one) in one warp
         pb.sorted.clear();
-        for (int k = 0; k < 16; k++)
+        for (int k = 0; k < 16; k++) {
+            const size_t first = pb.sorted.size();
             for (size_t i = 0; i < pb.bin.size(); i++)
                 if (pb.bin[i] == k) pb.sorted.push_back((int)i);
+            std::stable_sort(pb.sorted.begin() + first, pb.sorted.end(),
+                             [&pb](int x, int y) { return pb.nuse_ref[x] > pb.nuse_ref[y]; });
+        }
     }
     rc = upload_pairs(s, true);
     if (rc) return cleanup(rc);
@@ -1209,6 +1357,8 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_multi) cudaFree(s->d_multi);
     if (s->d_D32) cudaFree(s->d_D32);
     if (s->d_F32) cudaFree(s->d_F32);
+    if (s->d_perm) cudaFree(s->d_perm);
+    if (s->d_Dint) cudaFree(s->d_Dint);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1243,8 +1393,8 @@ int vlx_b200_screener_pair_info(const vlx_b200_screener* s, int* info, double* m
             info[6 * k + 1] = pb.bin[i];
             info[6 * k + 2] = pb.la;
             info[6 * k + 3] = pb.lb;
-            info[6 * k + 4] = s->shells[pb.pairs[i].first].ao0;
-            info[6 * k + 5] = s->shells[pb.pairs[i].second].ao0;
+            info[6 * k + 4] = s->shells[pb.pairs[i].first].ao0_ref;
+            info[6 * k + 5] = s->shells[pb.pairs[i].second].ao0_ref;
             maxv[k] = pb.maxv[i];
         }
     }
@@ -1308,8 +1458,6 @@ int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int nde
     const int chunk = std::min(ndens, vlx::kMaxDens);
     if (s->nmulti < chunk) {
         if (s->d_multi) cudaFree(s->d_multi);
-    if (s->d_D32) cudaFree(s->d_D32);
-    if (s->d_F32) cudaFree(s->d_F32);
         s->d_multi = nullptr;
         VLX_CUDA(cudaMalloc(&s->d_multi, 2 * (size_t)chunk * std::max<size_t>(bytes, 8)));
         s->nmulti = chunk;
@@ -1336,7 +1484,15 @@ int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int nde
         L.dens.n = nd;
         bool chunk_any = false;
         for (int d = 0; d < nd; d++) {
-            VLX_CUDA(cudaMemcpyAsync(dD + d * nn, densities[c0 + d], bytes, cudaMemcpyHostToDevice, s->stream));
+            if (s->permuted) {
+                // through the accumulator slot into the internal order
+                VLX_CUDA(cudaMemcpyAsync(dA + d * nn, densities[c0 + d], bytes, cudaMemcpyHostToDevice, s->stream));
+                permute_in_kernel<<<s->nao, 256, 0, s->stream>>>(dA + d * nn, dD + d * nn, s->d_perm, s->nao);
+                VLX_CUDA(cudaGetLastError());
+                acc.kernel_launches++;
+            } else {
+                VLX_CUDA(cudaMemcpyAsync(dD + d * nn, densities[c0 + d], bytes, cudaMemcpyHostToDevice, s->stream));
+            }
             L.dens.D[d] = dD + d * nn;
             L.dens.F[d] = dA + d * nn;
             L.dens.cj[d] = cj[c0 + d];
@@ -1353,12 +1509,12 @@ int vlx_b200_fock_build_multi(vlx_b200_screener* s, int rank, int nodes, int nde
             acc.prim_quartets += ts->prim_quartets;
         }
         for (int d = 0; d < nd; d++) {
-            // the density slot takes the output once the class kernels are done (stream order)
-            if (symmetric) {
-                const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-                symmetrize_kernel<<<grid, blk, 0, s->stream>>>(dA + d * nn, dD + d * nn, s->nao);
-                VLX_CUDA(cudaGetLastError());
-                acc.kernel_launches++;
+            // the density slot takes the output (caller's order) once the
+            // class kernels are done (stream order)
+            if (symmetric || s->permuted) {
+                const int rc = write_fock(s, dA + d * nn, nullptr, dD + d * nn, symmetric != 0, s->stream,
+                                          &acc.kernel_launches);
+                if (rc) return rc;
                 VLX_CUDA(cudaMemcpyAsync(focks_out[c0 + d], dD + d * nn, bytes, cudaMemcpyDeviceToHost, s->stream));
             } else {
                 VLX_CUDA(cudaMemcpyAsync(focks_out[c0 + d], dA + d * nn, bytes, cudaMemcpyDeviceToHost, s->stream));
@@ -1408,19 +1564,22 @@ int vlx_b200_set_partition(vlx_b200_screener* s, int mode)
 }  // extern "C"
 
 // ------------------------------------------------------------------ allocation-free build
-// Scratch of vlx_b200_fock_build_noalloc: the FP64 Fock accumulator (at most
-// VLX_B200_NOALLOC_MAX_NAO^2 values, 8 MiB) and the work-queue heads of the
-// class launches live in static device arrays instead of cudaMalloc'd buffers.
-// Every device that loads the library holds these 8 MiB until the process
-// exits; all calls share them.
+// Scratch of vlx_b200_fock_build_noalloc: the FP64 Fock accumulator and the
+// density in the internal AO order (at most VLX_B200_NOALLOC_MAX_NAO^2 values,
+// 8 MiB, each) and the work-queue heads of the class launches live in static
+// device arrays instead of cudaMalloc'd buffers.  Every device that loads the
+// library holds these 16 MiB until the process exits; all calls share them.
 namespace {
 
 constexpr int kNoallocMaxClasses = 64;
 static __device__ __align__(256) double g_noalloc_acc[(size_t)VLX_B200_NOALLOC_MAX_NAO * VLX_B200_NOALLOC_MAX_NAO];
+// the density in the screener's internal AO order
+static __device__ __align__(256) double g_noalloc_dint[(size_t)VLX_B200_NOALLOC_MAX_NAO * VLX_B200_NOALLOC_MAX_NAO];
 static __device__ __align__(256) int g_noalloc_heads[2 * kNoallocMaxClasses];  // FP64, then FP32 heads
 
 struct NoallocScratch {
     double* acc = nullptr;
+    double* dint = nullptr;
     int* heads = nullptr;
 };
 std::mutex g_noalloc_mutex;
@@ -1436,6 +1595,7 @@ int noalloc_scratch(int device, NoallocScratch* out)
         NoallocScratch sc;
         VLX_CUDA(cudaSetDevice(device));
         VLX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.acc), g_noalloc_acc));
+        VLX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.dint), g_noalloc_dint));
         VLX_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&sc.heads), g_noalloc_heads));
         it = g_noalloc.emplace(device, sc).first;
     }
@@ -1485,11 +1645,14 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
     // (the class launches clear their own queue heads, FP64 and FP32 blocks)
     VLX_CUDA(cudaMemsetAsync(sc.acc, 0, bytes, st));
     if (known && !ts->classes.empty()) {
+        const double* dI = nullptr;
+        rc = internal_density(s, d_density, st, &dI, nullptr, sc.dint);
+        if (rc) return rc;
         LaunchCtx L;
         L.blocks = s->d_blocks;
         L.glob = s->glob;
         L.counters = sc.heads;
-        L.mol.D = d_density;
+        L.mol.D = dI;
         L.mol.F = sc.acc;
         L.mol.nao = s->nao;
         for (int l = 0; l <= VLX_LMAX; l++) L.mol.nl[l] = s->nl[l];
@@ -1499,14 +1662,7 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
                          rs ? omega * omega : 0.0, ith, s->ith32, st, nullptr);
         if (rc) return rc;
     }
-    if (symmetric) {
-        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-        symmetrize_kernel<<<grid, blk, 0, st>>>(sc.acc, d_fock, s->nao);
-        VLX_CUDA(cudaGetLastError());
-    } else {
-        VLX_CUDA(cudaMemcpyAsync(d_fock, sc.acc, bytes, cudaMemcpyDeviceToDevice, st));
-    }
-    return VLX_B200_OK;
+    return write_fock(s, sc.acc, nullptr, d_fock, symmetric != 0, st, nullptr);
 }
 
 int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
@@ -1659,11 +1815,25 @@ int vlx_b200_compute_eri(vlx_b200_screener* s, int ith, double* eri_out)
     if (!rc) rc = build_tasks(s, ith, 0, 1, &ts);
     if (!rc) rc = enqueue_classes(s, ts, vlx::MODE_ERI, s->d_D, s->d_acc, d_eri, 0.0, 0.0, 0.0, ith, -1, s->stream,
                                   nullptr);
+    // the kernels scatter in the internal AO order: reorder into the caller's
+    double* d_out = d_eri;
+    if (!rc && s->permuted && n > 0) {
+        e = cudaMalloc(&d_out, bytes);
+        if (e != cudaSuccess) {
+            d_out = d_eri;
+            rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+        } else {
+            permute_eri_kernel<<<(unsigned)(n * n), 256, 0, s->stream>>>(d_eri, d_out, s->d_perm, (int)n);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
+        }
+    }
     if (!rc) {
-        e = cudaMemcpyAsync(eri_out, d_eri, bytes, cudaMemcpyDeviceToHost, s->stream);
+        e = cudaMemcpyAsync(eri_out, d_out, bytes, cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     }
+    if (d_out != d_eri) cudaFree(d_out);
     cudaFree(d_eri);
     return rc;
 }
@@ -1699,9 +1869,6 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     const bool dev_count = dscr_active(s);
     if (dev_count && s->nqstat < (int)(4 * nc)) {
         if (s->d_qstat) cudaFree(s->d_qstat);
-    if (s->d_multi) cudaFree(s->d_multi);
-    if (s->d_D32) cudaFree(s->d_D32);
-    if (s->d_F32) cudaFree(s->d_F32);
         s->d_qstat = nullptr;
         s->nqstat = std::max<int>(4 * (int)nc, 256);
         VLX_CUDA(cudaMalloc(&s->d_qstat, s->nqstat * sizeof(unsigned long long)));
@@ -1709,18 +1876,12 @@ int vlx_b200_fock_profile(vlx_b200_screener* s, const double* d_density, int sym
     if (dev_count) VLX_CUDA(cudaMemsetAsync(s->d_qstat, 0, 4 * nc * sizeof(unsigned long long), st));
     VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, bytes, st));
     const float* acc32 = nullptr;
-    rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, d_density, s->d_acc, nullptr,
-                         cj, ck, 0.0, ith, s->ith32, st, nullptr, &ev, dev_count ? s->d_qstat : nullptr, &acc32);
-    if (!rc && symmetric) {
-        const dim3 grid((s->nao + 31) / 32, (s->nao + 31) / 32), blk(32, 8);
-        symmetrize_kernel<<<grid, blk, 0, st>>>(s->d_acc, d_fock, s->nao, acc32);
-    } else if (!rc && acc32) {
-        const size_t nn = (size_t)s->nao * s->nao;
-        add_acc32_kernel<<<(unsigned)std::min<size_t>((nn + 255) / 256, 4096), 256, 0, st>>>(s->d_acc, acc32, d_fock,
-                                                                                             nn);
-    } else if (!rc) {
-        cudaMemcpyAsync(d_fock, s->d_acc, bytes, cudaMemcpyDeviceToDevice, st);
-    }
+    const double* dI = nullptr;
+    rc = internal_density(s, d_density, st, &dI, nullptr);
+    if (!rc)
+        rc = enqueue_classes(s, ts, symmetric ? vlx::MODE_FOCK_SYM : vlx::MODE_FOCK_GEN, dI, s->d_acc, nullptr, cj,
+                             ck, 0.0, ith, s->ith32, st, nullptr, &ev, dev_count ? s->d_qstat : nullptr, &acc32);
+    if (!rc) rc = write_fock(s, s->d_acc, acc32, d_fock, symmetric != 0, st, nullptr);
     cudaError_t e = cudaStreamSynchronize(st);
     if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
     std::vector<unsigned long long> qs(4 * nc, 0);
@@ -1833,8 +1994,12 @@ int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F)
 // replayed.  No counterpart in the reference, whose FockDriver builds one
 // molecule per call.
 
+// perm (may be null): the molecules' internal-to-caller AO permutations,
+// molecule k's at perm + aooff[k].
 __global__ void symmetrize_batch_kernel(const double* __restrict__ acc, double* __restrict__ out,
-                                        const long long* __restrict__ off, const int* __restrict__ nao)
+                                        const long long* __restrict__ off, const int* __restrict__ nao,
+                                        const int* __restrict__ perm = nullptr,
+                                        const int* __restrict__ aooff = nullptr)
 {
     __shared__ double tile[32][33];
     const int mol = blockIdx.z;
@@ -1848,10 +2013,44 @@ __global__ void symmetrize_batch_kernel(const double* __restrict__ acc, double* 
         tile[ty][tx] = (r < n && c < n) ? acc[(size_t)r * n + c] : 0.0;
     }
     __syncthreads();
+    const int* pm = perm ? perm + aooff[mol] : nullptr;
     for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
         const int i = by * 32 + ty, j = bx * 32 + tx;
-        if (i < n && j < n) out[(size_t)i * n + j] = acc[(size_t)i * n + j] + tile[tx][ty];
+        if (i < n && j < n) {
+            const double v = acc[(size_t)i * n + j] + tile[tx][ty];
+            if (pm)
+                out[(size_t)__ldg(pm + i) * n + __ldg(pm + j)] = v;
+            else
+                out[(size_t)i * n + j] = v;
+        }
     }
+}
+
+// Batched densities into the molecules' internal AO orders: molecule
+// blockIdx.y, row blockIdx.x.
+__global__ void permute_in_batch_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                        const long long* __restrict__ off, const int* __restrict__ nao,
+                                        const int* __restrict__ perm, const int* __restrict__ aooff)
+{
+    const int mol = blockIdx.y, i = blockIdx.x, n = nao[mol];
+    if (i >= n) return;
+    const int* pm = perm + aooff[mol];
+    const double* row = src + off[mol] + (size_t)__ldg(pm + i) * n;
+    double* o = dst + off[mol] + (size_t)i * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) o[j] = row[__ldg(pm + j)];
+}
+
+// Batched general accumulators back into the caller's AO orders.
+__global__ void permute_out_batch_kernel(const double* __restrict__ acc, double* __restrict__ dst,
+                                         const long long* __restrict__ off, const int* __restrict__ nao,
+                                         const int* __restrict__ perm, const int* __restrict__ aooff)
+{
+    const int mol = blockIdx.y, i = blockIdx.x, n = nao[mol];
+    if (i >= n) return;
+    const int* pm = perm + aooff[mol];
+    const double* a = acc + off[mol] + (size_t)i * n;
+    double* row = dst + off[mol] + (size_t)__ldg(pm + i) * n;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) row[__ldg(pm + j)] = a[j];
 }
 
 struct vlx_b200_batch {
@@ -1866,6 +2065,13 @@ struct vlx_b200_batch {
     long long* d_off = nullptr;
     int* d_nao = nullptr;
     double* d_acc = nullptr;
+    // the molecules' internal AO orders (permuted: some screener's order
+    // differs from the caller's): concatenated permutations, their offsets,
+    // and the packed densities in the internal orders
+    bool permuted = false;
+    int* d_perm = nullptr;
+    int* d_aooff = nullptr;
+    double* d_dint = nullptr;
     int* d_counters = nullptr;
     int ncounters = 0;
     std::vector<TaskSet> merged;    // one per ithreshold
@@ -1961,10 +2167,17 @@ int batch_tasks(vlx_b200_batch* b, int ith, TaskSet** out)
 
 // The launch sequence of one batched build on `st`.
 int batch_enqueue(vlx_b200_batch* b, TaskSet* ts, bool known, int symmetric, double cj, double ck, double omega2,
-                  double* d_focks, cudaStream_t st, long long* launches)
+                  const double* d_densities, double* d_focks, cudaStream_t st, long long* launches)
 {
     const long long total = b->off.back();
     VLX_CUDA(cudaMemsetAsync(b->d_acc, 0, (size_t)std::max<long long>(total, 1) * sizeof(double), st));
+    const dim3 rows((unsigned)std::max(b->max_nao, 1), (unsigned)b->mols.size());
+    if (known && b->permuted) {
+        permute_in_batch_kernel<<<rows, 256, 0, st>>>(d_densities, b->d_dint, b->d_off, b->d_nao, b->d_perm,
+                                                      b->d_aooff);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    }
     if (known) {
         LaunchCtx L;
         L.blocks = b->d_blocks;
@@ -1978,7 +2191,13 @@ int batch_enqueue(vlx_b200_batch* b, TaskSet* ts, bool known, int symmetric, dou
     if (symmetric) {
         const int t = (b->max_nao + 31) / 32;
         const dim3 grid(t, t, (unsigned)b->mols.size()), blk(32, 8);
-        symmetrize_batch_kernel<<<grid, blk, 0, st>>>(b->d_acc, d_focks, b->d_off, b->d_nao);
+        symmetrize_batch_kernel<<<grid, blk, 0, st>>>(b->d_acc, d_focks, b->d_off, b->d_nao,
+                                                      b->permuted ? b->d_perm : nullptr, b->d_aooff);
+        VLX_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+    } else if (b->permuted) {
+        permute_out_batch_kernel<<<rows, 256, 0, st>>>(b->d_acc, d_focks, b->d_off, b->d_nao, b->d_perm,
+                                                       b->d_aooff);
         VLX_CUDA(cudaGetLastError());
         if (launches) (*launches)++;
     } else {
@@ -2018,10 +2237,13 @@ int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screen
     b->mols.assign(screeners, screeners + n);
     b->off.assign(n + 1, 0);
     std::vector<PairBlockDev> blocks;
-    std::vector<int> nao(n);
+    std::vector<int> nao(n), perm, aooff(n + 1, 0);
     for (int k = 0; k < n; k++) {
         const vlx_b200_screener* s = screeners[k];
         nao[k] = s->nao;
+        perm.insert(perm.end(), s->perm.begin(), s->perm.end());
+        aooff[k + 1] = aooff[k] + s->nao;
+        b->permuted = b->permuted || s->permuted;
         b->max_nao = std::max(b->max_nao, s->nao);
         b->off[k + 1] = b->off[k] + (long long)s->nao * s->nao;
         for (PairBlockDev d : s->h_blocks) {
@@ -2044,6 +2266,13 @@ int vlx_b200_batch_create(vlx_b200_batch** out, vlx_b200_screener* const* screen
         VLX_CUDA(cudaMalloc(&b->d_nao, n * sizeof(int)));
         VLX_CUDA(cudaMemcpy(b->d_nao, nao.data(), n * sizeof(int), cudaMemcpyHostToDevice));
         VLX_CUDA(cudaMalloc(&b->d_acc, (size_t)std::max<long long>(b->off.back(), 1) * sizeof(double)));
+        VLX_CUDA(cudaMalloc(&b->d_aooff, (n + 1) * sizeof(int)));
+        VLX_CUDA(cudaMemcpy(b->d_aooff, aooff.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        if (b->permuted) {
+            VLX_CUDA(cudaMalloc(&b->d_perm, std::max<size_t>(perm.size(), 1) * sizeof(int)));
+            VLX_CUDA(cudaMemcpy(b->d_perm, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice));
+            VLX_CUDA(cudaMalloc(&b->d_dint, (size_t)std::max<long long>(b->off.back(), 1) * sizeof(double)));
+        }
         return VLX_B200_OK;
     };
     const int rc = setup();
@@ -2067,6 +2296,9 @@ int vlx_b200_batch_destroy(vlx_b200_batch* b)
     cudaFree(b->d_off);
     cudaFree(b->d_nao);
     cudaFree(b->d_acc);
+    cudaFree(b->d_aooff);
+    if (b->d_perm) cudaFree(b->d_perm);
+    if (b->d_dint) cudaFree(b->d_dint);
     if (b->d_counters) cudaFree(b->d_counters);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -2103,7 +2335,7 @@ int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int 
         std::vector<vlx::MolDev> h(b->mols.size());
         for (size_t k = 0; k < h.size(); k++) {
             const vlx_b200_screener* s = b->mols[k];
-            h[k].D = d_densities + b->off[k];
+            h[k].D = (b->permuted ? b->d_dint : d_densities) + b->off[k];
             h[k].F = b->d_acc + b->off[k];
             h[k].nao = s->nao;
             for (int l = 0; l <= VLX_LMAX; l++) h[k].nl[l] = s->nl[l];
@@ -2113,7 +2345,7 @@ int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int 
     }
     long long launches = 0;
     if (!use_graph) {
-        rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_focks, st, &launches);
+        rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_densities, d_focks, st, &launches);
         if (rc) return rc;
     } else {
         const bool same = b->exec && b->key_D == d_densities && b->key_F == d_focks && b->key_sym == symmetric &&
@@ -2123,7 +2355,7 @@ int vlx_b200_batch_fock_build(vlx_b200_batch* b, const double* d_densities, int 
             batch_release_graph(b);
             cudaGraph_t graph = nullptr;
             VLX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
-            rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_focks, b->stream, &launches);
+            rc = batch_enqueue(b, ts, known, symmetric, cj, ck, omega2, d_densities, d_focks, b->stream, &launches);
             const cudaError_t ec = cudaStreamEndCapture(b->stream, &graph);
             if (rc) {
                 if (graph) cudaGraphDestroy(graph);
@@ -2189,6 +2421,9 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
     int rc = ensure_buffers(s);
     if (rc) return rc;
+    const double* dI = nullptr;  // the density in the internal AO order
+    rc = internal_density(s, d_density, st, &dI, nullptr);
+    if (rc) return rc;
     const int ith32_saved = s->ith32;
     s->ith32 = -1;
     s->class_seg.clear();
@@ -2196,7 +2431,6 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
     const size_t ncand = sizeof(kTuneCandidates) / sizeof(kTuneCandidates[0]);
     std::map<int, std::vector<float>> times;  // class key -> ms per candidate
     std::map<int, int> kind;                  // class key -> 1 if warp-cooperative
-    double* dF = s->d_F;
     for (size_t k = 0; k < ncand && !rc; k++) {
         s->seg_try_compiled = kTuneCandidates[k].compiled;
         s->seg_try_coop = kTuneCandidates[k].coop;
@@ -2211,7 +2445,7 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
             VLX_CUDA(cudaEventCreate(&e.second));
         }
         VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, (size_t)s->nao * s->nao * sizeof(double), st));
-        rc = enqueue_classes(s, ts, vlx::MODE_FOCK_SYM, d_density, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
+        rc = enqueue_classes(s, ts, vlx::MODE_FOCK_SYM, dI, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
                              nullptr,
                              &ev);
         const cudaError_t e = cudaStreamSynchronize(st);
@@ -2232,7 +2466,6 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
             cudaEventDestroy(x.second);
         }
     }
-    (void)dF;
     s->seg_try_compiled = s->seg_try_coop = 0;
     // the tuning task sets are not needed any more
     for (auto it = s->tasksets.begin(); it != s->tasksets.end();) {
@@ -2276,7 +2509,7 @@ int vlx_b200_autotune(vlx_b200_screener* s, const double* d_density, int ith, vo
             VLX_CUDA(cudaEventCreate(&e.second));
         }
         VLX_CUDA(cudaMemsetAsync(s->d_acc, 0, (size_t)s->nao * s->nao * sizeof(double), st));
-        rc = enqueue_classes(s, tsb, vlx::MODE_FOCK_SYM, d_density, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
+        rc = enqueue_classes(s, tsb, vlx::MODE_FOCK_SYM, dI, s->d_acc, nullptr, 4.0, -1.0, 0.0, ith, -1, st,
                              nullptr, &ev);
         const cudaError_t e = cudaStreamSynchronize(st);
         if (!rc && e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));

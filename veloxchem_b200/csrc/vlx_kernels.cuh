@@ -36,11 +36,15 @@ __device__ __forceinline__ void addF(T* F, int nao, int r, int c, T v)
 // accumulated in one orientation and the caller adds the transpose at the end.
 // T = double, or float for the FP32 digestion of FP32 quartets into the
 // separate FP32 accumulator of a density-screened build (FP32 copy of D).
-template <int NA, int NB, int NC, int ND, int MODE, typename T>
+// JS > 0: jacc is the lane's part of the work item's F_PQ accumulator, element
+// e at jacc[JS e] (JS = 1: the lane's registers; JS = 32: the lane's column of
+// a per-warp shared-memory array); F_PQ is then reduced over the lanes once
+// per work item (flush_jpq) instead of once per step.
+template <int NA, int NB, int NC, int ND, int MODE, typename T, int JS = 0>
 __device__ __forceinline__ void digest_t(const T* f, const T s, const int lane, const int p0, const int nlp,
                                          const int q0, const int nlq, const int r0, const int nlr, const int s0,
                                          const int nls, const T* __restrict__ D, T* F, const int nao, const T cjw,
-                                         const T ckw)
+                                         const T ckw, T* jacc = nullptr)
 {
     const T cj = cjw * s, ck = ckw * s;
     if (cjw != T(0)) {
@@ -59,10 +63,14 @@ __device__ __forceinline__ void digest_t(const T* f, const T s, const int lane, 
                         v = fma(f[((i * NB + j) * NC + k) * ND + l], d, v);
                     }
                 }
-                v = warp_sum(v * cj);
-                if (lane == ((i * NB + j) & 31)) {
-                    addF(F, nao, p0 + i * nlp, q0 + j * nlq, v);
-                    if (MODE == MODE_FOCK_GEN) addF(F, nao, q0 + j * nlq, p0 + i * nlp, v);
+                if constexpr (JS > 0) {
+                    jacc[JS * (i * NB + j)] = fma(v, cj, jacc[JS * (i * NB + j)]);
+                } else {
+                    v = warp_sum(v * cj);
+                    if (lane == ((i * NB + j) & 31)) {
+                        addF(F, nao, p0 + i * nlp, q0 + j * nlq, v);
+                        if (MODE == MODE_FOCK_GEN) addF(F, nao, q0 + j * nlq, p0 + i * nlp, v);
+                    }
                 }
             }
         }
@@ -168,12 +176,34 @@ __device__ __forceinline__ void digest_t(const T* f, const T s, const int lane, 
     }
 }
 
-template <int NA, int NB, int NC, int ND, int MODE>
+template <int NA, int NB, int NC, int ND, int MODE, int JS = 0>
 __device__ __forceinline__ void digest(const double* f, const double s, const int lane, const int p0, const int nlp,
                                        const int q0, const int nlq, const int r0, const int nlr, const int s0,
-                                       const int nls, const MolDev& m, const double cjw, const double ckw)
+                                       const int nls, const MolDev& m, const double cjw, const double ckw,
+                                       double* jacc = nullptr)
 {
-    digest_t<NA, NB, NC, ND, MODE, double>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m.D, m.F, m.nao, cjw, ckw);
+    digest_t<NA, NB, NC, ND, MODE, double, JS>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m.D, m.F, m.nao,
+                                               cjw, ckw, jacc);
+}
+
+// End of a work item with item-level F_PQ accumulation (element e of the
+// lane's part at jl[JS e]): sum each element over the lanes and add it once
+// (and its transpose for a general density).
+template <int NA, int NB, int JS>
+__device__ __forceinline__ void flush_jpq(const double* jl, const int lane, const int mode, const int p0,
+                                          const int nlp, const int q0, const int nlq, const MolDev& m)
+{
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < NA * NB; e++) {
+        const double v = warp_sum(jl[JS * e]);
+        if (lane == (e & 31)) {
+            const int i = e / NB, j = e % NB;
+            addF(m.F, m.nao, p0 + i * nlp, q0 + j * nlq, v);
+            if ((mode & 3) == MODE_FOCK_GEN) addF(m.F, m.nao, q0 + j * nlq, p0 + i * nlp, v);
+        }
+    }
+    __syncwarp();
 }
 
 // Scatter one unique spherical quartet into the dense ERI tensor (all eight
@@ -209,11 +239,17 @@ constexpr int kWarpsPerBlock = 4;
 //   BlocksHint::value  minimum resident 128-thread blocks per SM the class's
 //                      register allocation must allow (0: no minimum);
 //   StageBra::value    stage the bra primitive records in shared memory per
-//                      work item (PairViewS).
+//                      work item (PairViewS);
+//   AccumulateJ::value where the plain kernel sums the F_PQ (J) elements of
+//                      a work item: 0 per step (warp sum and atomic add per
+//                      step), 1 per work item in registers, 2 per work item in
+//                      a per-warp shared-memory array.
 template <int LA, int LB, int LC, int LD>
 struct BlocksHint;
 template <int LA, int LB, int LC, int LD>
 struct StageBra;
+template <int LA, int LB, int LC, int LD>
+struct AccumulateJ;
 
 // One step of a work item: lane evaluates ket pair jj of kb against the bra
 // pair (act = false: an idle lane, which computes and contributes nothing)
@@ -227,7 +263,8 @@ __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, 
                                              const PairBlockDev& bb, const PairBlockDev& kb, const int bbi,
                                              const int kbi, const WorkItem& w, const PairView& bra, const MolDev& m,
                                              const int p0, const int q0, const double s_bra, const int jj,
-                                             const bool act, const double* sboys, const void* sbra)
+                                             const bool act, const double* sboys, const void* sbra,
+                                             double* jacc = nullptr)
 {
     using C = EriClass<LA, LB, LC, LD>;
     constexpr int NA = 2 * LA + 1, NB = 2 * LB + 1, NC = 2 * LC + 1, ND = 2 * LD + 1;
@@ -297,10 +334,14 @@ __device__ __forceinline__ void quartet_step(const FockArgs& a, const int mode, 
         if (r0 == s0) s *= 0.5;
         if (bbi == kbi && jj == w.bra) s *= 0.5;
         if constexpr (!EXT) {
+            constexpr int acc = AccumulateJ<LA, LB, LC, LD>::value;
+            constexpr int js = acc == 1 ? 1 : (acc == 2 ? 32 : 0);
             if (dmode == MODE_FOCK_SYM)
-                digest<NA, NB, NC, ND, MODE_FOCK_SYM>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+                digest<NA, NB, NC, ND, MODE_FOCK_SYM, js>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj,
+                                                          a.ck, jacc);
             else
-                digest<NA, NB, NC, ND, MODE_FOCK_GEN>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj, a.ck);
+                digest<NA, NB, NC, ND, MODE_FOCK_GEN, js>(f, s, lane, p0, nlp, q0, nlq, r0, nlr, s0, nls, m, a.cj,
+                                                          a.ck, jacc);
             return;
         }
         // one density, or each density of a multi-density build in turn
@@ -334,6 +375,10 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
     __shared__ double sboys[BOYS_NINT * BOYS_NCOEF];
     // per warp: the staged bra primitive records of the current work item
     __shared__ __align__(16) double sbra_all[StageBra<LA, LB, LC, LD>::value ? kWarpsPerBlock * kStageBraMax * 10 : 2];
+    // per warp: the plain kernels' F_PQ accumulator of the current work item
+    // (AccumulateJ 2)
+    constexpr int NAB = (2 * LA + 1) * (2 * LB + 1);
+    __shared__ double sjacc[(!EXT && AccumulateJ<LA, LB, LC, LD>::value == 2) ? kWarpsPerBlock * 32 * NAB : 1];
     const bool f32 = (mode & MODE_F32) != 0;
     if (f32) {
         float* sf = reinterpret_cast<float*>(sboys);
@@ -373,11 +418,28 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
         int k0, k1;
         if constexpr (!EXT) {
             item_range(a, bb, kb, w, f32, k0, k1);
+            // the lane's part of the item's F_PQ accumulator when the item
+            // digests J into a Fock matrix (AccumulateJ)
+            constexpr int acc = AccumulateJ<LA, LB, LC, LD>::value;
+            double jreg[acc == 1 ? NAB : 1];
+            double* jl = nullptr;
+            if constexpr (acc != 0) {
+                if ((mode & 3) != MODE_ERI && a.cj != 0.0 && k0 < k1) {
+                    jl = (acc == 1) ? jreg : sjacc + (threadIdx.x >> 5) * (32 * NAB) + lane;
+#pragma unroll
+                    for (int e = 0; e < NAB; e++) jl[(acc == 1 ? 1 : 32) * e] = 0.0;
+                }
+            }
             for (int j0 = k0; j0 < k1; j0 += 32) {
                 const int j = j0 + lane;
                 const bool act = j < k1;
                 quartet_step<LA, LB, LC, LD, false>(a, mode, f32, lane, bb, kb, bbi, kbi, w, bra, m, p0, q0, s_bra,
-                                                    act ? j : (k1 - 1), act, sboys, sbra);
+                                                    act ? j : (k1 - 1), act, sboys, sbra, jl);
+            }
+            if constexpr (acc != 0) {
+                if (jl)
+                    flush_jpq<2 * LA + 1, 2 * LB + 1, (acc == 1 ? 1 : 32)>(jl, lane, mode, p0, m.nl[LA], q0,
+                                                                          m.nl[LB], m);
             }
             continue;
         }

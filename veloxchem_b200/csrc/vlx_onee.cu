@@ -60,13 +60,9 @@ __device__ void boys_all(const int M, const double T, double* F, const double* _
         const int it = (int)(T * (double)BOYS_INV_H);
         const double x = fma(2.0 * BOYS_INV_H, T, -(double)(2 * it + 1));
         const double* c = tab + ((size_t)(M * BOYS_NINT + it)) * BOYS_NCOEF;
-        double b1 = 0.0, b2 = 0.0;
-        for (int j = BOYS_NCOEF - 1; j >= 1; j--) {
-            const double b0 = fma(2.0 * x, b1, __ldg(c + j) - b2);
-            b2 = b1;
-            b1 = b0;
-        }
-        F[M] = fma(x, b1, __ldg(c) - b2);
+        double p = __ldg(c + BOYS_NCOEF - 1);
+        for (int j = BOYS_NCOEF - 2; j >= 0; j--) p = fma(p, x, __ldg(c + j));
+        F[M] = p;
         const double et = exp(-T);
         for (int m = M - 1; m >= 0; m--) F[m] = fma(2.0 * T, F[m + 1], et) / (double)(2 * m + 1);
     } else {
