@@ -47,7 +47,9 @@ def _headers_digest(abi=False):
     for p in sorted(files):
         if p.exists():
             h.update(p.read_bytes())
-    h.update(' '.join(NVCC_FLAGS).encode())
+    # flags with the tree's own location left out, so that a copy of the tree
+    # keeps its objects
+    h.update(' '.join(f.replace(str(PKG.parent), '<root>') for f in NVCC_FLAGS).encode())
     return h.hexdigest()[:16]
 
 

@@ -281,16 +281,26 @@ class ClassGen:
         w('                const double WQx = rh * PQx, WQy = rh * PQy, WQz = rh * PQz;')
         w('                const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);')
         w('                double F[%d];' % (L + 1))
+        # F_m scaled by the primitive prefactor inside the Boys evaluation;
         # erf-attenuated operator: F_m(T) -> s^(2m+1) F_m(s^2 T), s^2 = om2 / (om2 + rho)
-        w('                const double s2 = (om2 > 0.0) ? om2 / (om2 + rho) : 1.0;')
-        w('                boys_function_tab<%d>(T * s2, F, btab);' % L)
-        w('                double pref = kab * kcd * r;')
-        w('                if (om2 > 0.0) pref *= sqrt(s2);')
-        w('                #pragma unroll')
-        w('                for (int m = 0; m <= %d; m++) {' % L)
-        w('                    F[m] *= pref;')
-        w('                    if (om2 > 0.0) pref *= s2;')
+        w('                double Tb = T;')
+        w('                double sc = kab * kcd * r;')
+        w('                double s2 = 1.0;')
+        w('                if (om2 > 0.0) {')
+        w('                    s2 = om2 / (om2 + rho);')
+        w('                    Tb = T * s2;')
+        w('                    sc *= sqrt(s2);')
         w('                }')
+        w('                boys_scaled<%d>(Tb, sc, F, btab);' % L)
+        if L > 0:
+            w('                if (om2 > 0.0) {')
+            w('                    double sm = s2;')
+            w('                    #pragma unroll')
+            w('                    for (int m = 1; m <= %d; m++) {' % L)
+            w('                        F[m] *= sm;')
+            w('                        sm *= s2;')
+            w('                    }')
+            w('                }')
         w('                (void)WPx; (void)WPy; (void)WPz; (void)WQx; (void)WQy; (void)WQz;')
         w('                (void)QDx; (void)QDy; (void)QDz; (void)PBx; (void)PBy; (void)PBz;')
         w('                (void)hiz; (void)hie; (void)hizh; (void)rz; (void)rh;')
@@ -571,8 +581,9 @@ def to_f32(method_lines):
         t = t.replace('double* __restrict__ out', 'float* __restrict__ out')
         t = t.replace('const double ', 'const float ').replace('double c_', 'float c_').replace('double F[', 'float F[')
         t = t.replace('double h_', 'float h_')
-        t = t.replace('boys_function_tab<', 'boys_function_tab_f<').replace('rsqrt(', 'rsqrtf(')
-        t = re.sub(r'(?<![r\w])sqrt\(', 'sqrtf(', t).replace('double pref', 'float pref')
+        t = t.replace('boys_scaled<', 'boys_scaled_f<').replace('rsqrt(', 'rsqrtf(')
+        t = re.sub(r'(?<![r\w])sqrt\(', 'sqrtf(', t)
+        t = re.sub(r'\bdouble (Tb|sc|s2|sm)\b', r'float \1', t)
         if not t.lstrip().startswith('//'):
             t = _FLOAT_LITERAL.sub(lambda m: m.group(1) + 'f', t)
         out.append(t)

@@ -26,7 +26,7 @@ __device__ __forceinline__ T ldD(const T* __restrict__ D, int nao, int r, int c)
 template <typename T>
 __device__ __forceinline__ void addF(T* F, int nao, int r, int c, T v)
 {
-    atomicAdd(F + (size_t)r * nao + c, v);
+    red_add(F + (size_t)r * nao + c, v);
 }
 
 // J/K digestion of the spherical block f[((i NB + j) NC + k) ND + l] of one

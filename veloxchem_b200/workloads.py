@@ -83,7 +83,7 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=T
                                        'table_driven': p['table_driven'], 'ms': p['device_ms'],
                                        'quartets': p['shell_quartets'], 'prim_quartets': p['prim_quartets'],
                                        'tflops': p['flops'] / max(p['device_ms'], 1e-9) / 1e9} for p in prof],
-                                     key=lambda r: -r['ms'])[:20]}
+                                     key=lambda r: -r['ms'])}
     dmax = float(d.abs().max())
     out['mixed'] = []
     for cut in cutoffs:
