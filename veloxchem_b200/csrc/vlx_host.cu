@@ -361,6 +361,20 @@ __global__ void shell_dmax_kernel(const double* __restrict__ D, const int nao, c
     dsh[idx] = __double2float_ru(m);
 }
 
+// Row maxima of the shell-block maxima (one thread per shell A): row[A] =
+// max_B dsh[A nsh + B], and row[nsh] = the maximum of all (cleared before;
+// non-negative floats order like their bit patterns).
+__global__ void shell_dmax_rows_kernel(const float* __restrict__ dsh, const int nsh, float* __restrict__ row)
+{
+    const int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= nsh) return;
+    const float* r = dsh + (size_t)A * nsh;
+    float m = 0.0f;
+    for (int B = 0; B < nsh; B++) m = fmaxf(m, r[B]);
+    row[A] = m;
+    atomicMax(reinterpret_cast<int*>(row + nsh), __float_as_int(m));
+}
+
 template <int M>
 __global__ void boys_test_kernel(const double* T, double* F, int n, const double* tab)
 {
@@ -475,6 +489,7 @@ struct vlx_b200_screener {
     double dscr_fp32 = 0.0, dscr_skip = 0.0;
     bool fp32_digest = false;    // FP32 quartets of density-screened builds digest in FP32 (set_fp32_digestion)
     float* d_dsh = nullptr;      // nsh x nsh shell-block max |D| of the build's density
+    float* d_dsh_row = nullptr;  // its row maxima and overall maximum (nsh + 1)
     int2* d_shinfo = nullptr;    // per shell: AO index of component 0, angular momentum
     unsigned long long* d_qstat = nullptr;  // profiled builds: [class][FP64, FP32][quartets, primitive quartets]
     int nqstat = 0;
@@ -889,6 +904,7 @@ struct LaunchCtx {
     const vlx::MolDev* mols = nullptr;
     // per-quartet density screening (dsh != nullptr): FockArgs::dsh, tau_skip, tau32
     const float* dsh = nullptr;
+    const float* dsh_row = nullptr;
     int nsh = 0;
     float tau_skip = 0.0f, tau32 = 0.0f;
     unsigned long long* qstat = nullptr;  // [class][FP64, FP32][2] quartet counters (profiled builds)
@@ -924,6 +940,7 @@ int enqueue_ctx(const LaunchCtx& L, TaskSet* ts, int mode, double* eri, double c
     a.ith = std::min(ith, ts->ith);
     a.ith32 = L.dsh ? -1 : ith32;
     a.dsh = L.dsh;
+    a.dsh_row = L.dsh_row;
     a.nsh = L.nsh;
     a.dens = L.dens;
     a.D32 = L.D32;
@@ -978,6 +995,7 @@ int prepare_dscr(vlx_b200_screener* s, const double* dD, cudaStream_t st)
     const int nsh = (int)s->shells.size();
     if (!s->d_dsh) {
         VLX_CUDA(cudaMalloc(&s->d_dsh, (size_t)nsh * nsh * sizeof(float)));
+        VLX_CUDA(cudaMalloc(&s->d_dsh_row, (size_t)(nsh + 1) * sizeof(float)));
         std::vector<int2> info(nsh);
         for (int i = 0; i < nsh; i++) info[i] = make_int2(s->shells[i].ao0, s->shells[i].l);
         VLX_CUDA(cudaMalloc(&s->d_shinfo, nsh * sizeof(int2)));
@@ -986,6 +1004,9 @@ int prepare_dscr(vlx_b200_screener* s, const double* dD, cudaStream_t st)
     const long long n = (long long)nsh * nsh;
     const int4 nl = make_int4(s->nl[0], s->nl[1], s->nl[2], s->nl[3]);
     shell_dmax_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dD, s->nao, s->d_shinfo, nsh, nl, s->d_dsh);
+    VLX_CUDA(cudaGetLastError());
+    VLX_CUDA(cudaMemsetAsync(s->d_dsh_row + nsh, 0, sizeof(float), st));
+    shell_dmax_rows_kernel<<<(unsigned)((nsh + 127) / 128), 128, 0, st>>>(s->d_dsh, nsh, s->d_dsh_row);
     VLX_CUDA(cudaGetLastError());
     return VLX_B200_OK;
 }
@@ -1012,8 +1033,9 @@ int enqueue_classes(vlx_b200_screener* s, TaskSet* ts, int mode, const double* d
     if (mode != vlx::MODE_ERI && dscr_active(s)) {
         const int rc = prepare_dscr(s, dD, st);
         if (rc) return rc;
-        if (launches) (*launches)++;
+        if (launches) (*launches) += 2;
         L.dsh = s->d_dsh;
+        L.dsh_row = s->d_dsh_row;
         L.nsh = (int)s->shells.size();
         L.tau_skip = (float)s->dscr_skip;
         L.tau32 = (float)s->dscr_fp32;
@@ -1352,6 +1374,7 @@ int vlx_b200_screener_destroy(vlx_b200_screener* s)
     if (s->d_acc) cudaFree(s->d_acc);
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->d_dsh) cudaFree(s->d_dsh);
+    if (s->d_dsh_row) cudaFree(s->d_dsh_row);
     if (s->d_shinfo) cudaFree(s->d_shinfo);
     if (s->d_qstat) cudaFree(s->d_qstat);
     if (s->d_multi) cudaFree(s->d_multi);

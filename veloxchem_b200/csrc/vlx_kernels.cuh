@@ -456,6 +456,7 @@ __device__ __forceinline__ void quartet_body(const FockArgs& a, const int mode)
             Q = __ldg(bb.sh + bb.npairs + w.bra);
             qpq = __ldg(bb.q + w.bra);
             dpq = __ldg(a.dsh + (size_t)P * a.nsh + Q);
+            k1 = density_ket_end(a, P, Q, qpq, dpq, kb, f32, k1);
         }
         // steps of 32 kets; with density screening the kets this launch keeps
         // are first compacted into full steps (order preserved)

@@ -93,6 +93,7 @@ struct FockArgs {
     // d the shell-block maxima of |D|; quartets below tau_skip are skipped,
     // those below tau32 are the FP32 launch's, the rest the FP64 launch's
     const float* dsh;         // nsh x nsh, max over the two orientations of the block
+    const float* dsh_row;     // per shell the maximum of its row of dsh, then the maximum of all (nsh + 1)
     int nsh;
     float tau_skip, tau32;
     unsigned long long* qstat;  // [2] quartets and primitive quartets evaluated by the launch (nullptr: off)

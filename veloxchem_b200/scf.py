@@ -170,6 +170,12 @@ class ScfRestrictedDriver:
         # the early builds' FP32 quartets digest in FP32 (their Fock matrices
         # are replaced by the switch build); the later builds digest in FP64
         self.early_fp32_digestion = True
+        # full builds after the early phase, in mixed precision: when set, the
+        # quartets bounded below this cutoff are evaluated and digested in FP32
+        # (their rounding is ~6e-8 of contributions below the cutoff) and all
+        # others in FP64, in place of FP32 below fp32_cutoff with FP64
+        # digestion (None: the latter)
+        self.full_fp32_digestion_cutoff = None
         self.history = []
         self.timings = {}
 
@@ -328,8 +334,12 @@ class ScfRestrictedDriver:
                 F2e.copy_(F2e_prev)
                 F2e.add_(G)
             else:
+                if mixed and not early and self.full_fp32_digestion_cutoff is not None:
+                    cutoff = float(self.full_fp32_digestion_cutoff)
+                    screener.set_fp32_digestion(True)
                 screener.set_density_screening(cutoff, self._skip_factor(early, self.full_skip_factor) * 10.0 ** (-ith))
                 build(D, F2e, ith)
+                screener.set_fp32_digestion(early and self.early_fp32_digestion)
                 ith_used = ith
             torch.cuda.synchronize(dev)
             fock_ms += 1e3 * (time.perf_counter() - t0)

@@ -412,7 +412,8 @@ def c3scf_variants(variants, log=None):
         t0 = time.perf_counter()
         res = drv.compute(mol, bas, screener=scr)
         out[name] = {'attrs': attrs, 'wall_s': time.perf_counter() - t0, 'energy': res['scf_energy'],
-                     'iterations': res['iterations'], '_h': res['history']}
+                     'iterations': res['iterations'], 'converged': res['converged'], '_h': res['history'],
+                     'timings': dict(drv.timings)}
         say('%s: %d it, %.1f s' % (name, res['iterations'], out[name]['wall_s']))
     e_ref = out['plain']['energy']
     for r in out.values():
@@ -494,11 +495,10 @@ def main(argv=None):
         res = c4_headline()
     elif a.which == 'c3scf':
         import sys
-        res = c3scf_variants([('fast_pulay', dict(acc_type='diis')),
-                              ('plain_pulay', dict(fp32_cutoff=0.0, guess='sad', incremental=False,
-                                                   early_ithreshold=None, acc_type='diis')),
-                              ('fast', {}),
-                              ('fast_full_skip_1e-1', dict(full_skip_factor=1e-1))],
+        res = c3scf_variants([('fast', {}),
+                              ('fast_full_fp32_digestion_1e-8', dict(full_fp32_digestion_cutoff=1e-8)),
+                              ('fast_full_fp32_digestion_1e-7', dict(full_fp32_digestion_cutoff=1e-7)),
+                              ('fast_full_fp32_digestion_1e-6', dict(full_fp32_digestion_cutoff=1e-6))],
                              log=lambda m: print(m, file=sys.stderr, flush=True))
     elif a.which == 'onee':
         res = onee(a.cluster, a.basis, a.repeat)
