@@ -189,6 +189,27 @@ def test_early_loose_iterations_reach_the_reference_energy():
     assert res['history'][-1]['ithreshold'] == 12
 
 
+@pytest.mark.gpu
+def test_full_builds_with_fp32_digestion_reach_the_reference_energy():
+    """The fast configuration with FP32 evaluation and digestion of the
+    quartets bounded below 1e-6 in the full builds after the early phase
+    (full_fp32_digestion_cutoff), per-quartet density screening and
+    incremental builds: it converges to the reference energy."""
+    from veloxchem_b200.scf import ScfRestrictedDriver
+    mol, bas = _dimer()
+    drv = ScfRestrictedDriver()
+    drv.fp32_cutoff = 1e-4
+    drv.early_ithreshold = 8
+    drv.full_skip_factor = 1e-2
+    drv.early_skip_factor = 1e-1
+    drv.full_fp32_digestion_cutoff = 1e-6
+    res = drv.compute(mol, bas)
+    assert res['converged']
+    assert abs(res['scf_energy'] - REF_ENERGY) < 1e-8
+    # the switch build after the early phase is a mixed full build
+    assert any(not h['incremental'] and h['ithreshold'] > 8 and h['mixed'] for h in res['history'])
+
+
 def test_scf_threshold_schedule():
     """The reference's dynamic ERI threshold (ScfDriver._get_dyn_threshold:
     1e-10 for gradients >= 1, one decade tighter per decade of gradient, 1e-12

@@ -694,8 +694,11 @@ GROUPED = {(1, 2, 1, 2): 5, (1, 3, 0, 3): 5, (1, 3, 1, 1): 5, (1, 3, 1, 2): 6, (
 # spilling (measured 15-20% faster each); a minimum of 3 for the classes at
 # 250+ registers was measured neutral.  An explicit minimum of 1 is not the
 # same as none: it lets the compiler take far more registers (186 instead of
-# 72 for (sp|ss)).
-BLOCKS_HINT = {(1, 1, 0, 0): 4, (0, 1, 0, 1): 5, (0, 2, 0, 0): 5, (0, 1, 0, 0): 8, (1, 1, 0, 1): 4, (0, 2, 0, 1): 4}
+# 72 for (sp|ss)).  After the Fock additions became reductions without a
+# returned value, (pp|ss) 6, (sd|ss) 8 and (sp|sp) 6 measured 1-13% faster
+# than 4, 5 and 5; higher minimums for (sp|ss), (pp|sp) and (sd|sp) were
+# slower (up to 1.8x).
+BLOCKS_HINT = {(1, 1, 0, 0): 6, (0, 1, 0, 1): 6, (0, 2, 0, 0): 8, (0, 1, 0, 0): 8, (1, 1, 0, 1): 4, (0, 2, 0, 1): 4}
 
 # Classes whose bra primitive records are staged in shared memory per work
 # item: measured faster staged on the (H2O)32 / def2-SVP build ((ss|ss)

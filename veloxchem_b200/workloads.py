@@ -279,7 +279,8 @@ def _warm_fast_path(scr, d):
 
 
 def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5, 1e-4), max_fock_error=1e-6, scf=True, log=None,
-                full_skip_factor=1e-2, early_skip_factor=1e-1, fp32_cutoff=1e-4, acc_type='c2diis'):
+                full_skip_factor=1e-2, early_skip_factor=1e-1, fp32_cutoff=1e-4, acc_type='c2diis',
+                full_fp32_digestion_cutoff=1e-6):
     """The north-star comparison on (H2O)64 / def2-TZVP in one process:
 
     * builds: the plain FP64 2J-K build (device ms, CUDA events, best of 2
@@ -353,6 +354,7 @@ def c3_headline(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5, 1e-4), max_fock_error=1e-
             if inc:
                 drv.full_skip_factor = full_skip_factor
                 drv.early_skip_factor = early_skip_factor
+                drv.full_fp32_digestion_cutoff = full_fp32_digestion_cutoff
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             res = drv.compute(mol, bas, screener=scr)
@@ -401,7 +403,7 @@ def c3scf_variants(variants, log=None):
     _build_ms(scr, d, torch.empty_like(d), reps=0)  # work list of threshold 12
     _warm_fast_path(scr, d)
     base = dict(fp32_cutoff=1e-4, guess='learned', incremental=True, early_ithreshold=8, full_skip_factor=1e-2,
-                early_skip_factor=1e-1, acc_type='c2diis')
+                early_skip_factor=1e-1, acc_type='c2diis', full_fp32_digestion_cutoff=1e-6)
     out = {}
     for name, attrs in [('plain', dict(fp32_cutoff=0.0, guess='sad', incremental=False, acc_type='c2diis'))] + \
             list(variants):
@@ -496,9 +498,8 @@ def main(argv=None):
     elif a.which == 'c3scf':
         import sys
         res = c3scf_variants([('fast', {}),
-                              ('fast_full_fp32_digestion_1e-8', dict(full_fp32_digestion_cutoff=1e-8)),
-                              ('fast_full_fp32_digestion_1e-7', dict(full_fp32_digestion_cutoff=1e-7)),
-                              ('fast_full_fp32_digestion_1e-6', dict(full_fp32_digestion_cutoff=1e-6))],
+                              ('fast_fp64_full_digestion', dict(full_fp32_digestion_cutoff=None)),
+                              ('fast_full_fp32_digestion_1e-5', dict(full_fp32_digestion_cutoff=1e-5))],
                              log=lambda m: print(m, file=sys.stderr, flush=True))
     elif a.which == 'onee':
         res = onee(a.cluster, a.basis, a.repeat)
