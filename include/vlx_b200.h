@@ -255,6 +255,18 @@ int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const
                           const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
                           const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out);
 
+/* The same matrix written to device memory: d_out (nao_bra x nao_ket,
+ * row-major, reference AO order) on `device`, computed on `stream`
+ * (cudaStream_t, NULL = the legacy default stream); returns once the matrix
+ * is complete.  For callers that keep S, T, V on the GPU (the SCF driver),
+ * which saves the copy to the host and back.  Same reference counterparts as
+ * vlx_b200_one_electron. */
+int vlx_b200_one_electron_device(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                                 const int* bra_atom, const int* bra_l, const int* bra_nprim,
+                                 const double* bra_exps, const double* bra_coefs, int nsh_ket, const int* ket_atom,
+                                 const int* ket_l, const int* ket_nprim, const double* ket_exps,
+                                 const double* ket_coefs, double* d_out, void* stream);
+
 /* Boys function F_m(T) for n arguments as the device evaluates it
  * (host arrays T[n] in, F[n] out), for validation. */
 int vlx_b200_boys_device(int device, int m, int n, const double* T, double* F);

@@ -115,6 +115,20 @@ def test_one_electron_against_reference(basis):
 
 
 @pytest.mark.gpu
+def test_one_electron_device_output_matches_host_output():
+    """vlx_b200_one_electron_device (output in device memory, as the SCF
+    driver keeps S, T, V) gives the host-output entry's matrices."""
+    import torch
+    from veloxchem_b200 import _native as nat
+    mol, bas = _dimer()
+    n = bas.get_dimensions_of_basis()
+    for which in range(3):
+        out = torch.full((n, n), 7.0, dtype=torch.float64, device='cuda')
+        nat.one_electron_device(which, mol, bas, out)
+        assert np.max(np.abs(out.cpu().numpy() - nat.one_electron(which, mol, bas))) < 1e-14, which
+
+
+@pytest.mark.gpu
 def test_mixed_overlap_against_reference():
     from oracle.oracle import RefOracle
     from veloxchem_b200 import MolecularBasis

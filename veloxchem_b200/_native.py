@@ -50,6 +50,8 @@ SIGNATURES = {
     'vlx_b200_fp64_peak': (ctypes.c_int, [ctypes.c_int, _dp]),
     'vlx_b200_one_electron': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int,
                                              _ip, _ip, _ip, _dp, _dp, ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _dp]),
+    'vlx_b200_one_electron_device': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, _dp, ctypes.c_int,
+                                             _ip, _ip, _ip, _dp, _dp, ctypes.c_int, _ip, _ip, _ip, _dp, _dp, _vp, _vp]),
     'vlx_b200_set_fp32_threshold': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     'vlx_b200_set_density_screening': (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     'vlx_b200_set_fp32_digestion': (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -196,6 +198,23 @@ def one_electron(which, molecule, bra_basis, ket_basis=None, device=0):
     check(lib().vlx_b200_one_electron(int(device), int(which), len(z), iptr(z), dptr(xyz), len(ba), iptr(ba),
                                       iptr(bl), iptr(bn), dptr(f64(be)), dptr(f64(bc)), len(ka), iptr(ka), iptr(kl),
                                       iptr(kn), dptr(f64(ke)), dptr(f64(kc)), dptr(out)), 'one_electron')
+    return out
+
+
+def one_electron_device(which, molecule, bra_basis, out, device=0, stream=None):
+    """S, T or V of bra_basis into the device tensor ``out`` (float64,
+    nao x nao, contiguous) on torch's current stream (or ``stream``)."""
+    import torch
+    z = i32(molecule.get_element_ids())
+    xyz = f64(molecule.get_coordinates_in_bohr())
+    ba, bl, bn, be, bc = [a if a.dtype == np.float64 else i32(a) for a in bra_basis.shell_table()]
+    if stream is None:
+        stream = torch.cuda.current_stream(out.device).cuda_stream or 1
+    check(lib().vlx_b200_one_electron_device(int(device), int(which), len(z), iptr(z), dptr(xyz), len(ba),
+                                             iptr(ba), iptr(bl), iptr(bn), dptr(f64(be)), dptr(f64(bc)), len(ba),
+                                             iptr(ba), iptr(bl), iptr(bn), dptr(f64(be)), dptr(f64(bc)),
+                                             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream)),
+          'one_electron_device')
     return out
 
 

@@ -1688,12 +1688,13 @@ int vlx_b200_fock_build_noalloc(vlx_b200_screener* s, const double* d_density, i
     return write_fock(s, sc.acc, nullptr, d_fock, symmetric != 0, st, nullptr);
 }
 
-int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
-                          const int* bra_atom, const int* bra_l, const int* bra_nprim, const double* bra_exps,
-                          const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
-                          const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out)
+static int one_electron_impl(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                             const int* bra_atom, const int* bra_l, const int* bra_nprim, const double* bra_exps,
+                             const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
+                             const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out,
+                             double* d_out, cudaStream_t st)
 {
-    if (which < 0 || which > 2 || natoms < 1 || !Z || !xyz || nsh_bra < 1 || nsh_ket < 1 || !out)
+    if (which < 0 || which > 2 || natoms < 1 || !Z || !xyz || nsh_bra < 1 || nsh_ket < 1 || (!out && !d_out))
         return fail(VLX_B200_ERR_ARGUMENT, "one_electron: invalid arguments");
     DeviceGlobals* g = nullptr;
     int rc = device_globals(device, &g);
@@ -1771,24 +1772,50 @@ int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const
     if (!rc) rc = up(zc.data(), zc.size() * 8, &dz);
     if (!rc) rc = up(xyz, (size_t)natoms * 3 * 8, &dxyz);
     const size_t obytes = (size_t)hb.nao * hk.nao * sizeof(double);
-    if (!rc) {
+    if (!rc && d_out) {
+        dout = d_out;
+    } else if (!rc) {
         cudaError_t e = cudaMalloc(&dout, obytes);
         if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, cudaGetErrorString(e));
         else bufs.push_back(dout);
     }
     if (!rc) {
-        cudaMemset(dout, 0, obytes);
+        cudaMemsetAsync(dout, 0, obytes, st);
         // the same basis on both sides: S, T, V are symmetric, one triangle of shell pairs is evaluated
         const bool sym = hb.l == hk.l && hb.nprim == hk.nprim && hb.xyz == hk.xyz && hb.exps == hk.exps &&
                          hb.coefs == hk.coefs;
         vlx::launch_one_electron(which, sets[0], sets[1], sym ? 1 : 0, natoms, static_cast<const double*>(dz),
-                                 static_cast<const double*>(dxyz), g->boys, static_cast<double*>(dout), hk.nao, 0);
+                                 static_cast<const double*>(dxyz), g->boys, static_cast<double*>(dout), hk.nao, st);
         cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpy(out, dout, obytes, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && out) e = cudaMemcpyAsync(out, dout, obytes, cudaMemcpyDeviceToHost, st);
+        // the shell tables are freed below: the kernel has to be done with them
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = fail(VLX_B200_ERR_CUDA, std::string("one_electron: ") + cudaGetErrorString(e));
     }
     free_all();
     return rc;
+}
+
+int vlx_b200_one_electron(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                          const int* bra_atom, const int* bra_l, const int* bra_nprim, const double* bra_exps,
+                          const double* bra_coefs, int nsh_ket, const int* ket_atom, const int* ket_l,
+                          const int* ket_nprim, const double* ket_exps, const double* ket_coefs, double* out)
+{
+    if (!out) return fail(VLX_B200_ERR_ARGUMENT, "one_electron: invalid arguments");
+    return one_electron_impl(device, which, natoms, Z, xyz, nsh_bra, bra_atom, bra_l, bra_nprim, bra_exps, bra_coefs,
+                             nsh_ket, ket_atom, ket_l, ket_nprim, ket_exps, ket_coefs, out, nullptr, 0);
+}
+
+int vlx_b200_one_electron_device(int device, int which, int natoms, const int* Z, const double* xyz, int nsh_bra,
+                                 const int* bra_atom, const int* bra_l, const int* bra_nprim,
+                                 const double* bra_exps, const double* bra_coefs, int nsh_ket, const int* ket_atom,
+                                 const int* ket_l, const int* ket_nprim, const double* ket_exps,
+                                 const double* ket_coefs, double* d_out, void* stream)
+{
+    if (!d_out) return fail(VLX_B200_ERR_ARGUMENT, "one_electron_device: null output");
+    return one_electron_impl(device, which, natoms, Z, xyz, nsh_bra, bra_atom, bra_l, bra_nprim, bra_exps, bra_coefs,
+                             nsh_ket, ket_atom, ket_l, ket_nprim, ket_exps, ket_coefs, nullptr, d_out,
+                             static_cast<cudaStream_t>(stream));
 }
 
 int vlx_b200_set_density_screening(vlx_b200_screener* s, double fp32_cutoff, double skip_cutoff)

@@ -211,10 +211,13 @@ class ScfRestrictedDriver:
             raise ValueError('ScfRestrictedDriver: odd number of electrons')
         nocc = nelec // 2
         t0 = time.perf_counter()
-        S_host = nat.one_electron(0, molecule, ao_basis, None, self.device)
-        S = torch.from_numpy(S_host).to(dev)
-        T = torch.from_numpy(nat.one_electron(1, molecule, ao_basis, None, self.device)).to(dev)
-        V = torch.from_numpy(nat.one_electron(2, molecule, ao_basis, None, self.device)).to(dev)
+        # S, T, V computed into device tensors (vlx_b200_one_electron_device);
+        # the host copy of S is for the SAD and learned guesses
+        nao = ao_basis.get_dimensions_of_basis()
+        S, T, V = (torch.empty((nao, nao), dtype=torch.float64, device=dev) for _ in range(3))
+        for which, m in enumerate((S, T, V)):
+            nat.one_electron_device(which, molecule, ao_basis, m, self.device)
+        S_host = S.cpu().numpy()
         H = T + V
         self.timings['one_electron_s'] = time.perf_counter() - t0
         w, u = torch.linalg.eigh(S)
