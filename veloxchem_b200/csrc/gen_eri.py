@@ -712,9 +712,11 @@ STAGE_BRA = {(0, 0, 0, 0), (0, 1, 0, 0), (1, 1, 0, 0), (0, 2, 0, 0), (2, 2, 1, 2
 # one warp sum and atomic add per 32-ket step (absent: per step).  Chosen per
 # class from timings of all three forms on the (H2O)32 / def2-SVP and
 # (H2O)64 / def2-TZVP builds (gains 3-12% per class; (sp|ss), (sp|sp),
-# (ss|ss), (pd|pd), (pd|pp) measured neutral or slower and stay per step).
+# (ss|ss), (pd|pd), (pd|pp), (sf|sf), (sf|pp) measured neutral or slower and
+# stay per step).
 ACCUM_J = {(1, 1, 0, 1): 1, (1, 2, 0, 1): 2, (1, 1, 0, 0): 2, (0, 2, 0, 1): 2, (0, 2, 1, 1): 2, (0, 2, 0, 0): 2,
-           (1, 1, 1, 1): 2, (1, 2, 0, 2): 2, (1, 2, 0, 0): 1, (0, 3, 0, 1): 2, (0, 3, 1, 2): 1}
+           (1, 1, 1, 1): 2, (1, 2, 0, 2): 2, (1, 2, 0, 0): 1, (0, 3, 0, 1): 2, (0, 3, 1, 2): 1, (0, 3, 0, 0): 2,
+           (0, 3, 0, 2): 2}
 
 
 def class_parts(cls):
