@@ -56,7 +56,12 @@ def _build_ms(scr, d, f, reps=3, enqueue=None):
     return best
 
 
-def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=True, autotune=False):
+def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=True, autotune=False,
+       density_screening=None):
+    """(H2O)64 / def2-TZVP builds, per-class profile (every class), the mixed
+    cutoffs and the SCF variants.  density_screening = (fp32_cutoff,
+    skip_cutoff): profile the density-screened kernels instead of the plain
+    ones (vlx_b200_set_density_screening)."""
     from . import T4CScreener
     from . import _native as nat
     from .geometry import random_density
@@ -75,6 +80,9 @@ def c3(cutoffs=(1e-9, 1e-8, 1e-7, 1e-6, 1e-5), scf=True, variants=None, builds=T
         t0 = time.perf_counter()
         out['autotune'] = nat.autotune(scr, d.data_ptr(), 12)
         out['autotune_s'] = time.perf_counter() - t0
+    if density_screening is not None:
+        scr.set_density_screening(*density_screening)
+        out['density_screening'] = list(density_screening)
     t64 = _build_ms(scr, d, f64, reps=3 if builds else 0)
     prof = nat.fock_profile(scr, d.data_ptr(), f64.data_ptr(), '2jk', 1.0, 12)
     flops = sum(p['flops'] for p in prof)
@@ -486,6 +494,8 @@ def main(argv=None):
     ap.add_argument('--scf-variants', default=None, help='comma-separated subset of the C3 SCF variants')
     ap.add_argument('--no-builds', action='store_true', help='C3: skip the per-cutoff build table')
     ap.add_argument('--autotune', action='store_true', help='C3: autotune the classes first')
+    ap.add_argument('--density-screening', type=float, nargs=2, default=None, metavar=('FP32', 'SKIP'),
+                    help='C3: profile the density-screened kernels with these cutoffs')
     a = ap.parse_args(argv)
     if a.which == 'build':
         res = build(a.cluster, a.basis, a.repeat, a.fp32_cutoff)
@@ -507,7 +517,8 @@ def main(argv=None):
         res = guess(a.cluster, a.repeat)
     else:
         res = (c3(scf=not a.no_scf, variants=a.scf_variants.split(',') if a.scf_variants else None,
-                  builds=not a.no_builds, autotune=a.autotune) if a.which == 'c3'
+                  builds=not a.no_builds, autotune=a.autotune, density_screening=a.density_screening)
+               if a.which == 'c3'
                else (c4() if a.which == 'c4' else c2scf()))
     text = json.dumps(res, indent=1)
     if a.out:
