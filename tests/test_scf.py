@@ -163,6 +163,20 @@ def test_sad_density_is_a_valid_guess():
     # trace(D S) = number of alpha electrons of the neutral atoms
     assert abs(np.trace(D @ S) - mol.number_of_electrons() / 2) < 1e-10
     assert np.allclose(D, D.T)
+    # the driver projects once per element; every atom projected on its own
+    # gives the same density
+    s12 = nat.one_electron(0, mol, mini, bas)
+    ao1 = SadGuessDriver.ao_indices_of_atoms(mol, mini)
+    ao2 = SadGuessDriver.ao_indices_of_atoms(mol, bas)
+    c = np.zeros((S.shape[0], s12.shape[0]))
+    for a, z in enumerate(mol.get_element_ids()):
+        i1, i2 = ao1[a], ao2[a]
+        occ = np.array(SadGuessDriver.occupation_numbers(int(z)))
+        b22_inv = np.linalg.inv(S[np.ix_(i2, i2)])
+        m = s12[np.ix_(i1, i2)] @ b22_inv @ s12[np.ix_(i1, i2)].T
+        w, v = np.linalg.eigh(m)
+        c[np.ix_(i2, i1)] = b22_inv @ s12[np.ix_(i1, i2)].T @ ((v / np.sqrt(w)) @ v.T) * np.sqrt(occ)[None, :]
+    assert np.max(np.abs(D - c @ c.T)) < 1e-10
 
 
 @pytest.mark.gpu

@@ -92,21 +92,27 @@ class SadGuessDriver:
         ao1 = self.ao_indices_of_atoms(molecule, min_basis)
         ao2 = self.ao_indices_of_atoms(molecule, ao_basis)
         csad = np.zeros((s22.shape[0], s12.shape[0]))
+        # the projection uses only the atom's own overlap blocks, which are the
+        # same for every atom of one element: computed once per element
+        blocks = {}
         for a, z in enumerate(molecule.get_element_ids()):
             i1, i2 = ao1[a], ao2[a]
-            occ = np.array(self.occupation_numbers(int(z)))
-            if len(occ) != len(i1):
-                raise ValueError('SAD: minimal basis / occupation mismatch for element %d' % z)
-            b12 = s12[np.ix_(i1, i2)]
-            b22 = s22[np.ix_(i2, i2)]
-            w, v = np.linalg.eigh(b22)
-            b22_inv = (v / w) @ v.T
-            mat_a = b12.T
-            mat_m = mat_a.T @ b22_inv @ mat_a
-            w, v = np.linalg.eigh(mat_m)
-            m_invsqrt = (v / np.sqrt(w)) @ v.T
-            c2 = b22_inv @ mat_a @ m_invsqrt
-            csad[np.ix_(i2, i1)] = c2 * np.sqrt(occ)[None, :]
+            z = int(z)
+            if z not in blocks:
+                occ = np.array(self.occupation_numbers(z))
+                if len(occ) != len(i1):
+                    raise ValueError('SAD: minimal basis / occupation mismatch for element %d' % z)
+                b12 = s12[np.ix_(i1, i2)]
+                b22 = s22[np.ix_(i2, i2)]
+                w, v = np.linalg.eigh(b22)
+                b22_inv = (v / w) @ v.T
+                mat_a = b12.T
+                mat_m = mat_a.T @ b22_inv @ mat_a
+                w, v = np.linalg.eigh(mat_m)
+                m_invsqrt = (v / np.sqrt(w)) @ v.T
+                c2 = b22_inv @ mat_a @ m_invsqrt
+                blocks[z] = c2 * np.sqrt(occ)[None, :]
+            csad[np.ix_(i2, i1)] = blocks[z]
         # D = C C^T (nao x nao from nao x n_min: ~15 GFLOP for (H2O)64 /
         # def2-TZVP) on the GPU rather than in the host's BLAS
         torch = _torch()
